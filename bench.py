@@ -1,0 +1,356 @@
+"""Benchmark: 512^3 ComplexF32 C2C forward + inverse, Slab decomposition.
+
+One step = one forward 3-D FFT plus one inverse 3-D FFT of a 512^3
+ComplexF32 array (BASELINE config "3D C2C fft/ifft ComplexF32 512x512x512,
+iid standard-normal real/imag, decomp=Slab()"), inputs resident in HBM.
+
+value  : algorithmic GB/s = 2 transforms x 3 axis passes x (read + write of
+         the 1 GiB field) = 12.885 GB per step, / step time, summed over ranks.
+e2e    : the same bytes / the time of the public API call sequence with host
+         buffers: pinned H2D of the input, fft, ifft, D2H of the result.
+roofline: the slowest axis-pass kernel, timed alone with CUDA events on its
+         stream: 2 x 1 GiB per launch / mean launch time vs the measured
+         HBM copy bandwidth in MEASURED_PEAKS.json.
+cpu_baseline: the oracle's restatement of the reference CPU pipeline
+         (Blocks(N,N,64) slabs, per-chunk pocketfft with all host threads,
+         block redistribution), one forward+inverse of the same 512^3 field.
+
+--impl reference times that CPU pipeline alone (rank 0), one forward+inverse
+per step, and prints its own JSON line.
+
+Multi-GPU (torchrun): every rank transforms its own 512^3 field (weak
+scaling, replicas: no data-path collective); timing is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "daggerfft.jl_b200"))
+
+N = 512
+FIELD_BYTES = N ** 3 * 8                     # ComplexF32
+STEP_BYTES = 2 * 3 * 2 * FIELD_BYTES         # fwd + inv, 3 passes, read + write
+PASS_BYTES = 2 * FIELD_BYTES                 # one axis pass
+CPU_CHUNK = 64
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the axis-pass kernels from the committed ncu
+    summary (profiles/ncu_traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_pipeline_once(A, workers):
+    """One forward + inverse of the oracle's Slab pipeline on host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import dfft_oracle as oracle
+    oracle.WORKERS = workers
+    shape = A.shape
+    DA, DB = oracle.slab_layouts(shape, CPU_CHUNK, 1)
+    oracle.distribute(A, DA)
+    wsAB = [oracle.create_workspace(DA, DB, 0)]
+    wsBA = [oracle.create_workspace(DB, DA, 0)]
+    t0 = time.perf_counter()
+    oracle.fft_slab(DB, DA, wsAB, (oracle.FFT_(),) * 3, (1, 2, 3), precision="native")
+    DA.chunks = []
+    oracle.ifft_slab(DA, DB, wsBA, (oracle.IFFT_(),) * 3, (1, 2, 3), precision="native")
+    return time.perf_counter() - t0
+
+
+def host_input(seed=0):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    re = rng.standard_normal((N, N, N), dtype=np.float32)
+    im = rng.standard_normal((N, N, N), dtype=np.float32)
+    a = np.empty((N, N, N), dtype=np.complex64, order="F")
+    a.real = re
+    a.imag = im
+    return a
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import numpy as np  # noqa: F401
+    workers = os.cpu_count() or 1
+    A = host_input()
+    for _ in range(args.warmup):
+        cpu_pipeline_once(A, workers)
+    ts = [cpu_pipeline_once(A, workers) for _ in range(args.steps)]
+    t = sum(ts) / len(ts)
+    v = STEP_BYTES / t / 1e9
+    line = {
+        "impl": "reference", "metric": "512^3 C2C FFT GB/s (fwd+inv, algorithmic bytes)",
+        "value": round(v, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "complex64 (f32)", "data": "synthetic",
+        "config": {"workload": "512^3 ComplexF32 C2C fft+ifft, Slab(), Blocks(512,512,64)",
+                   "global_batch": 1, "seq_len": N, "parallelism": "host threads"},
+        "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": workers, "kind": "port",
+                         "sample": "one full 512^3 forward+inverse per step (oracle Slab pipeline, "
+                                   "pocketfft stand-in for FFTW)"},
+        "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gflops": round(5 * N ** 3 * 27 * 1e-9 / (t / 2), 2),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--method", default="plain", choices=["plain", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import numpy as np
+    import torch
+    import dfft
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+
+    stream = torch.cuda.current_stream(dev)
+    A_host = torch.from_numpy(np.ascontiguousarray(host_input(seed=rank).T)).pin_memory()  # (z,y,x) C = F(x,y,z)
+    out_host = torch.empty_like(A_host).pin_memory()
+    Ad = A_host.to(dev, non_blocking=False).permute(2, 1, 0)     # logical (x,y,z), column-major
+    Bd = dfft.empty_like_layout(Ad.shape, Ad.dtype, Ad)
+    Cd = dfft.empty_like_layout(Ad.shape, Ad.dtype, Ad)
+    decomp = dfft.Slab()
+    pf = dfft.get_or_create_gpu_plan(dfft.FFT(), Ad, (1, 2, 3), decomp=decomp, method=args.method)
+    pi = dfft.get_or_create_gpu_plan(dfft.IFFT(), Bd, (1, 2, 3), decomp=decomp, method=args.method)
+    launches_per_step = pf.launches + pi.launches
+
+    def step():
+        pf.execute(Ad, Bd, stream)
+        pi.execute(Bd, Cd, stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    try:
+        gid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        gid = str(local)
+    clocks = ClockSampler(gid)
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_ms = e0.elapsed_time(e1) / args.steps
+    if pg:
+        pg.barrier()
+    clk = clocks.stop()
+    if pg:
+        tt = torch.tensor([t_ms], device=dev)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = world * STEP_BYTES / (t_ms * 1e-3) / 1e9
+
+    # accuracy: round trip, and forward vs the FP64 path of this library
+    rt = float(torch.linalg.vector_norm(Cd - Ad) / torch.linalg.vector_norm(Ad))
+    A64 = Ad.to(torch.complex128)
+    F64 = dfft.fft(A64, decomp=decomp, dims=(1, 2, 3))
+    fwd_err = float(torch.linalg.vector_norm(Bd.to(torch.complex128) - F64) / torch.linalg.vector_norm(F64))
+    del A64, F64
+    torch.cuda.empty_cache()
+
+    # per-axis kernels timed alone (roofline of the dominant kernel)
+    per_axis = {}
+    for ax in (1, 2, 3):
+        p = dfft.gpu_plan_transform(dfft.FFT(), Ad, (ax,), decomp=decomp, method=args.method)
+        for _ in range(3):
+            p.execute(Ad, Bd, stream)
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        reps = 10
+        a0.record(stream)
+        for _ in range(reps):
+            p.execute(Ad, Bd, stream)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        per_axis[ax] = a0.elapsed_time(a1) / reps / p.launches
+        del p
+    dom_ax = max(per_axis, key=per_axis.get)
+    peak, peak_kind = measured_peak()
+    achieved = PASS_BYTES / (per_axis[dom_ax] * 1e-3) / 1e9
+    traffic = None
+    tr = ncu_traffic()
+    if tr and str(dom_ax) in tr.get("axis_pass_bytes", {}):
+        traffic = tr["axis_pass_bytes"][str(dom_ax)]
+
+    # end-to-end through the public API with host buffers
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    Ad_flat = Ad.permute(2, 1, 0)  # the C-ordered storage view matching A_host
+    Cd_flat = Cd.permute(2, 1, 0)
+    for _ in range(2):
+        Ad_flat.copy_(A_host, non_blocking=True)
+        step()
+        out_host.copy_(Cd_flat, non_blocking=True)
+    torch.cuda.synchronize()
+    ee0 = torch.cuda.Event(enable_timing=True)
+    ee1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(3, min(args.steps, 10))
+    ee0.record(stream)
+    for _ in range(e2e_steps):
+        Ad_flat.copy_(A_host, non_blocking=True)
+        step()
+        out_host.copy_(Cd_flat, non_blocking=True)
+    ee1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = ee0.elapsed_time(ee1) / e2e_steps
+    if pg:
+        tt = torch.tensor([e2e_ms], device=dev)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e = world * STEP_BYTES / (e2e_ms * 1e-3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        workers = os.cpu_count() or 1
+        a_np = A_host.numpy().T  # logical (x,y,z), Fortran order
+        t_cpu = cpu_pipeline_once(a_np, workers)
+        cpu = {"value": round(STEP_BYTES / t_cpu / 1e9, 3), "unit": "GB/s", "cores": workers,
+               "kind": "port",
+               "sample": "one 512^3 ComplexF32 forward+inverse (oracle Slab pipeline: Blocks(512,512,64) "
+                         "chunks, pocketfft per chunk with all host threads, block redistribution)"}
+
+    if pg:
+        pg.barrier()
+    if rank == 0:
+        line = {
+            "metric": "512^3 C2C FFT GB/s (fwd+inv, algorithmic bytes)",
+            "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(t_ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex64 (f32)",
+            "data": "synthetic",
+            "config": {"workload": "512^3 ComplexF32 C2C fft+ifft, decomp=Slab(), dims=(1,2,3)",
+                       "method": args.method, "global_batch": world, "seq_len": N,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs (1 GiB) larger than L2 (126 MB); no flush needed"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": traffic, "kernel": f"axis pass dim {dom_ax}",
+                         "per_axis_ms": {str(k): round(v, 4) for k, v in per_axis.items()},
+                         "step_frac_of_peak": round(value / world / peak, 4)},
+            "e2e": {"value": round(e2e, 2), "unit": "GB/s", "ms_per_step": round(e2e_ms, 3),
+                    "h2d_bytes_per_step": FIELD_BYTES, "d2h_bytes_per_step": FIELD_BYTES},
+            "cpu_baseline": cpu,
+            "gpu_launches": launches_per_step * args.steps,
+            "gflops": round(5 * N ** 3 * 27 * 1e-9 / (t_ms * 1e-3 / 2), 1),
+            "errors": {"roundtrip_rel_l2": rt, "fwd_rel_l2_vs_fp64": fwd_err},
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

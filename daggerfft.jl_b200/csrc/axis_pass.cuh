@@ -1,0 +1,417 @@
+// One batched 1-D transform pass along one axis of a column-major array.
+//
+// Data model.  A pass transforms Q independent "columns" of FFT length L.
+// Column q is split as (qi, qo) = (q % I, q / I); element k of column q of a
+// side (input or output) sits at  p[qi*si + qo*so + k*sk]  of that side.  One
+// kernel therefore serves the contiguous axis (I = 1: a column is a whole
+// pencil) and the strided axes (I = product of the faster dims: consecutive
+// columns are adjacent in memory, so the strided loads coalesce).
+//
+// Work split.  A CTA owns C consecutive columns and runs P threads per column.
+// With cfast the column index sits in the fastest thread bits (strided axes:
+// a warp reads adjacent elements of one row of the tile); otherwise the
+// butterfly index does (contiguous axis: a warp reads one pencil).
+//
+// Algorithm.  Stockham autosort FFT, stages s = 0..nst-1 with radix R_s and
+// Ns = R_0*...*R_{s-1}.  Butterfly j of stage s reads k = j + r*(L/R_s),
+// multiplies by w_{Ns*R}^{(j mod Ns)*r}, runs a radix-R_s codelet and writes
+// k' = (j - j mod Ns)*R_s + j mod Ns + r*Ns.  The first stage reads straight
+// from global memory and the last stage writes straight to global memory (both
+// index patterns are unit-stride in j), so a pass costs one read and one write
+// of HBM; the nst-1 intermediate exchanges go through shared memory.
+//
+// The inverse transform runs the forward kernel on conjugated data
+// (IDFT(x) = conj(DFT(conj(x)))), with the 1/L scale folded into the store.
+//
+// Two kernels share the stage body:
+//   * axis_pass_static<T, FAST_IO, LB, L, P, R...>: radices known at compile
+//     time, every stage inlined and constant-folded (the hot path);
+//   * axis_pass_dynamic<T, EMAX>: radices read from the descriptor, one
+//     out-of-line function per radix (any 13-smooth length).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "codelets.cuh"
+
+namespace dfft {
+
+constexpr int kMaxStages = 16;
+
+// How a side of a pass maps FFT elements to memory.
+enum IoKind : int {
+  IO_CPLX = 0,       // complex elements
+  IO_REAL_PAIR = 1,  // real pairs: z_m <-> (x_{2m}, x_{2m+1})
+  IO_REAL = 2,       // load (x_k, 0) / store Re z_k
+  IO_HERM_PAIR = 3,  // load only: even-length C2R pre-pass (real length 2n)
+  IO_HERM_FULL = 4,  // load only: odd-length C2R, Hermitian mirror
+  IO_TRUNC = 5,      // store only: complex, keep k <= n
+  IO_R2R = 6         // FFTW r2r kind `r2r` on real data of extent n
+};
+
+// FFTW r2r kind numbers (fftw_r2r_kind).
+enum : int { K_DHT = 2, K_REDFT00 = 3, K_REDFT01 = 4, K_REDFT10 = 5, K_REDFT11 = 6,
+             K_RODFT00 = 7, K_RODFT01 = 8, K_RODFT10 = 9, K_RODFT11 = 10 };
+
+struct IoAny {
+  void* p;
+  long long si, so, sk;
+  int kind;          // IoKind
+  int r2r;           // FFTW kind for IO_R2R
+  int n;             // logical extent (see the kinds)
+  const void* w;     // twiddle table for the kinds that need one
+};
+
+struct PassDesc {
+  int L;                    // transform length of this pass
+  int nst;                  // number of Stockham stages (dynamic kernel only)
+  int radix[kMaxStages];
+  int ns[kMaxStages];
+  int tws[kMaxStages];
+  int P;                    // threads per column
+  int C;                    // columns per CTA
+  int ld;                   // shared-memory elements reserved per column
+  int inverse;              // 1: conjugate on load and on store
+  int cfast;                // thread -> (column, butterfly) mapping
+  int epi;                  // 1: R2C half-length post-pass on the way out
+  long long Q;              // number of columns
+  long long I;              // column split q -> (q % I, q / I)
+  double scale;             // multiplier applied at the store
+  const void* tw;           // L entries exp(-2 pi i m / L)
+  const void* tw2;          // epi: L+1 entries exp(-2 pi i m / (2L))
+  IoAny in, out;
+};
+
+// Bank-conflict swizzle for the shared-memory exchange: one pad element per
+// 128 bytes of complex data.
+template <typename V> __device__ __forceinline__ int swz(int k) {
+  return sizeof(V) == 8 ? k + (k >> 4) : k + (k >> 3);
+}
+
+template <typename V> __device__ __forceinline__ V ldg_c(const V* p) { return __ldg(p); }
+
+// ---------------------------------------------------------------------------
+// Element access for every side kind.  The r2r maps (FFTW kinds, all
+// unnormalised) express each kind as one complex FFT:
+//   kind      FFT length  input map                            output
+//   REDFT10   N           v_k = x_{2k} | x_{2N-2k-1}            Y_k = 2 Re(e^{-i pi k/2N} V_k)
+//   RODFT10   N           as REDFT10 on (-1)^n x_n              Y_{N-1-k} = that value
+//   REDFT01   N, inverse  V_n = e^{i pi n/2N}(x_n - i x_{N-n})  y_{2m} | y_{2N-2m-1} = Re v_m
+//   RODFT01   N, inverse  as REDFT01 on x reversed              times (-1)^k
+//   REDFT11   2N          x_n e^{-i pi n/2N}, zero-padded       Y_k = 2 Re(e^{-i pi (2k+1)/4N} X_k)
+//   RODFT11   2N          as REDFT11 on x reversed              times (-1)^k
+//   REDFT00   2(N-1)      even extension                        Y_k = Re X_k
+//   RODFT00   2(N+1)      odd extension [0, x, 0, -rev(x)]      Y_k = -Im X_{k+1}
+//   DHT       N           x_n                                   Y_k = Re X_k - Im X_k
+// ---------------------------------------------------------------------------
+
+template <typename T>
+__device__ __forceinline__ typename cvec<T>::type load_elem(const IoAny& io, long long b, int k) {
+  typedef typename cvec<T>::type V;
+  const T z = (T)0;
+  switch (io.kind) {
+    case IO_CPLX:
+      return reinterpret_cast<const V*>(io.p)[b + k * io.sk];
+    case IO_REAL_PAIR: {
+      const T* p = reinterpret_cast<const T*>(io.p);
+      if (io.sk == 1) return *reinterpret_cast<const V*>(p + b + 2 * (long long)k);
+      return mk<V>(p[b + (2 * k) * io.sk], p[b + (2 * k + 1) * io.sk]);
+    }
+    case IO_REAL:
+      return mk<V>(reinterpret_cast<const T*>(io.p)[b + k * io.sk], z);
+    case IO_HERM_PAIR: {
+      // Z'_k = (A + B) + i conj(w^k) (A - B), A = X_k, B = conj(X_{n-k});
+      // the inverse FFT of Z' (length n) interleaves to 2n * x.
+      const V* p = reinterpret_cast<const V*>(io.p);
+      V A = p[b + k * io.sk];
+      V B = cconj(p[b + (io.n - k) * io.sk]);
+      if (k == 0) { A.y = (T)0; B.y = (T)0; }  // c2r ignores Im X_0 and Im X_{n}
+      V wk = cconj(ldg_c(reinterpret_cast<const V*>(io.w) + k));
+      return cadd(cadd(A, B), cmul_pi(cmul(wk, csub(A, B))));
+    }
+    case IO_HERM_FULL: {
+      const V* p = reinterpret_cast<const V*>(io.p);
+      if (k == 0) return mk<V>(p[b].x, z);  // c2r ignores Im X_0
+      if (2 * k <= io.n) return p[b + k * io.sk];
+      return cconj(p[b + (io.n - k) * io.sk]);
+    }
+    default: {  // IO_R2R
+      const T* p = reinterpret_cast<const T*>(io.p);
+      const V* w = reinterpret_cast<const V*>(io.w);
+      const int N = io.n;
+      const long long sk = io.sk;
+      switch (io.r2r) {
+        case K_REDFT10:
+        case K_RODFT10: {
+          const int n = (2 * k < N) ? 2 * k : 2 * N - 2 * k - 1;
+          T v = p[b + n * sk];
+          if (io.r2r == K_RODFT10 && (n & 1)) v = -v;
+          return mk<V>(v, z);
+        }
+        case K_REDFT01:
+        case K_RODFT01: {
+          const bool rev = (io.r2r == K_RODFT01);
+          const T a = p[b + (rev ? N - 1 - k : k) * sk];
+          const T c = (k == 0) ? z : p[b + (rev ? k - 1 : N - k) * sk];
+          return cmul(ldg_c(w + k), mk<V>(a, -c));
+        }
+        case K_REDFT11:
+        case K_RODFT11: {
+          if (k >= N) return mk<V>(z, z);
+          const T a = p[b + (io.r2r == K_RODFT11 ? N - 1 - k : k) * sk];
+          const V t = ldg_c(w + k);
+          return mk<V>(a * t.x, a * t.y);
+        }
+        case K_REDFT00: {
+          const int n = (k < N) ? k : 2 * (N - 1) - k;
+          return mk<V>(p[b + n * sk], z);
+        }
+        case K_RODFT00: {
+          if (k == 0 || k == N + 1) return mk<V>(z, z);
+          if (k <= N) return mk<V>(p[b + (k - 1) * sk], z);
+          return mk<V>(-p[b + (2 * N + 1 - k) * sk], z);
+        }
+        default:  // K_DHT
+          return mk<V>(p[b + k * sk], z);
+      }
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void store_elem(const IoAny& io, long long b, int k,
+                                           typename cvec<T>::type v, T s) {
+  typedef typename cvec<T>::type V;
+  switch (io.kind) {
+    case IO_CPLX:
+      reinterpret_cast<V*>(io.p)[b + k * io.sk] = cscale(v, s);
+      return;
+    case IO_TRUNC:
+      if (k <= io.n) reinterpret_cast<V*>(io.p)[b + k * io.sk] = cscale(v, s);
+      return;
+    case IO_REAL_PAIR: {
+      T* p = reinterpret_cast<T*>(io.p);
+      if (io.sk == 1) { *reinterpret_cast<V*>(p + b + 2 * (long long)k) = cscale(v, s); return; }
+      p[b + (2 * k) * io.sk] = v.x * s;
+      p[b + (2 * k + 1) * io.sk] = v.y * s;
+      return;
+    }
+    case IO_REAL:
+      reinterpret_cast<T*>(io.p)[b + k * io.sk] = v.x * s;
+      return;
+    default: {  // IO_R2R
+      T* p = reinterpret_cast<T*>(io.p);
+      const V* w = reinterpret_cast<const V*>(io.w);
+      const int N = io.n;
+      const long long sk = io.sk;
+      switch (io.r2r) {
+        case K_REDFT10:
+        case K_RODFT10: {
+          const V t = ldg_c(w + k);
+          p[b + (io.r2r == K_RODFT10 ? N - 1 - k : k) * sk] = (T)2 * (v.x * t.x - v.y * t.y) * s;
+          return;
+        }
+        case K_REDFT01:
+        case K_RODFT01: {
+          const int n = (2 * k < N) ? 2 * k : 2 * N - 2 * k - 1;
+          T y = v.x * s;
+          if (io.r2r == K_RODFT01 && (n & 1)) y = -y;
+          p[b + n * sk] = y;
+          return;
+        }
+        case K_REDFT11:
+        case K_RODFT11: {
+          if (k >= N) return;
+          const V t = ldg_c(w + k);
+          T y = (T)2 * (v.x * t.x - v.y * t.y) * s;
+          if (io.r2r == K_RODFT11 && (k & 1)) y = -y;
+          p[b + k * sk] = y;
+          return;
+        }
+        case K_REDFT00:
+          if (k < N) p[b + k * sk] = v.x * s;
+          return;
+        case K_RODFT00:
+          if (k >= 1 && k <= N) p[b + (k - 1) * sk] = -v.y * s;
+          return;
+        default:  // K_DHT
+          p[b + k * sk] = (v.x - v.y) * s;
+          return;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stage body.
+// ---------------------------------------------------------------------------
+
+// BMAX: upper bound on butterflies per thread; in the static kernel it is
+// exactly ceil((L/R)/P), in the dynamic kernel EMAX/R.
+template <typename T, int R, int BMAX, bool FAST_IO>
+__device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int Ns, int ts,
+                                           bool first, bool last, int t,
+                                           typename cvec<T>::type* col,
+                                           const typename cvec<T>::type* tw,
+                                           long long ib, long long ob, bool cv) {
+  typedef typename cvec<T>::type V;
+  const int Lr = L / R;
+  const bool to_global = last && !d.epi;
+  V v[BMAX][R];
+#pragma unroll
+  for (int b = 0; b < BMAX; ++b) {
+    const int j = t + b * P;
+    if (j < Lr) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int k = j + r * Lr;
+        if (first) {
+          V x;
+          if (!cv) x = mk<V>((T)0, (T)0);
+          else if (FAST_IO) x = reinterpret_cast<const V*>(d.in.p)[ib + k * d.in.sk];
+          else x = load_elem<T>(d.in, ib, k);
+          if (d.inverse) x.y = -x.y;
+          v[b][r] = x;
+        } else {
+          v[b][r] = col[swz<V>(k)];
+        }
+      }
+    }
+  }
+  if (!first) __syncthreads();
+#pragma unroll
+  for (int b = 0; b < BMAX; ++b) {
+    const int j = t + b * P;
+    if (j < Lr) {
+      const int jm = j % Ns;
+      if (!first) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[b][r] = cmul(v[b][r], ldg_c(tw + jm * r * ts));
+      }
+      Dft<R>::run(v[b]);
+      const int o0 = (j - jm) * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int k = o0 + r * Ns;
+        if (to_global) {
+          if (cv) {
+            V y = v[b][r];
+            if (d.inverse) y.y = -y.y;
+            if (FAST_IO) reinterpret_cast<V*>(d.out.p)[ob + k * d.out.sk] = cscale(y, (T)d.scale);
+            else store_elem<T>(d.out, ob, k, y, (T)d.scale);
+          }
+        } else {
+          col[swz<V>(k)] = v[b][r];
+        }
+      }
+    }
+  }
+  if (!to_global) __syncthreads();
+}
+
+// Shared prologue: thread -> (column, butterfly lane), column base offsets.
+struct ColCtx {
+  int c, t;
+  bool cv;
+  long long ib, ob;
+};
+
+__device__ __forceinline__ ColCtx col_ctx(const PassDesc& d, int P) {
+  ColCtx x;
+  const int tid = threadIdx.x;
+  if (d.cfast) { x.c = tid % d.C; x.t = tid / d.C; }
+  else { x.t = tid % P; x.c = tid / P; }
+  const long long q = (long long)blockIdx.x * d.C + x.c;
+  x.cv = q < d.Q;
+  const long long qi = x.cv ? q % d.I : 0;
+  const long long qo = x.cv ? q / d.I : 0;
+  x.ib = qi * d.in.si + qo * d.in.so;
+  x.ob = qi * d.out.si + qo * d.out.so;
+  return x;
+}
+
+// R2C post-pass over the half-length spectrum Z (length M) in shared memory:
+// X_k = E_k + w^k O_k, E = (Z_k + conj Z_{M-k})/2, O = -i (Z_k - conj Z_{M-k})/2.
+template <typename T>
+__device__ __forceinline__ void r2c_epilogue(const PassDesc& d, int P, const ColCtx& x,
+                                             const typename cvec<T>::type* col) {
+  typedef typename cvec<T>::type V;
+  const int M = d.L;
+  const V* w2 = reinterpret_cast<const V*>(d.tw2);
+  if (!x.cv) return;
+  for (int k = x.t; k <= M; k += P) {
+    V zk = col[swz<V>(k == M ? 0 : k)];
+    V zm = cconj(col[swz<V>(k == 0 ? 0 : M - k)]);
+    V e = cscale(cadd(zk, zm), (T)0.5);
+    V o = cscale(cmul_mi(csub(zk, zm)), (T)0.5);
+    store_elem<T>(d.out, x.ob, k, cadd(e, cmul(ldg_c(w2 + k), o)), (T)d.scale);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Static-plan kernel.
+// ---------------------------------------------------------------------------
+
+template <typename T, int L, int P, bool FAST_IO, int NS, int S, int R, int... Rest>
+__device__ __forceinline__ void static_stages(const PassDesc& d, int t, typename cvec<T>::type* col,
+                                              const typename cvec<T>::type* tw, long long ib,
+                                              long long ob, bool cv) {
+  constexpr int Lr = L / R;
+  constexpr int BM = (Lr + P - 1) / P;
+  constexpr int TS = L / (NS * R);
+  stage_body<T, R, BM, FAST_IO>(d, L, P, NS, TS, S == 0, sizeof...(Rest) == 0, t, col, tw, ib, ob,
+                                cv);
+  if constexpr (sizeof...(Rest) > 0)
+    static_stages<T, L, P, FAST_IO, NS * R, S + 1, Rest...>(d, t, col, tw, ib, ob, cv);
+}
+
+template <typename T, bool FAST_IO, int LB, int L, int P, int... Rs>
+__global__ void __launch_bounds__(LB) axis_pass_static(const PassDesc d) {
+  typedef typename cvec<T>::type V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* sm = reinterpret_cast<V*>(smem_raw);
+  const ColCtx x = col_ctx(d, P);
+  V* col = sm + x.c * d.ld;
+  const V* tw = reinterpret_cast<const V*>(d.tw);
+  static_stages<T, L, P, FAST_IO, 1, 0, Rs...>(d, x.t, col, tw, x.ib, x.ob, x.cv);
+  if (!FAST_IO && d.epi) r2c_epilogue<T>(d, P, x, col);
+}
+
+// ---------------------------------------------------------------------------
+// Dynamic-plan kernel (fallback for lengths without a static plan).
+// ---------------------------------------------------------------------------
+
+template <typename T, int R, int EMAX>
+__device__ __noinline__ void dyn_stage(const PassDesc& d, int s, int t, typename cvec<T>::type* col,
+                                       const typename cvec<T>::type* tw, long long ib, long long ob,
+                                       bool cv) {
+  stage_body<T, R, EMAX / R, false>(d, d.L, d.P, d.ns[s], d.tws[s], s == 0, s == d.nst - 1, t, col,
+                                    tw, ib, ob, cv);
+}
+
+template <typename T, int EMAX>
+__global__ void __launch_bounds__(1024) axis_pass_dynamic(const PassDesc d) {
+  typedef typename cvec<T>::type V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* sm = reinterpret_cast<V*>(smem_raw);
+  const ColCtx x = col_ctx(d, d.P);
+  V* col = sm + x.c * d.ld;
+  const V* tw = reinterpret_cast<const V*>(d.tw);
+  for (int s = 0; s < d.nst; ++s) {
+    switch (d.radix[s]) {
+      case 1: dyn_stage<T, 1, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 2: dyn_stage<T, 2, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 3: dyn_stage<T, 3, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 4: dyn_stage<T, 4, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 5: dyn_stage<T, 5, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 7: dyn_stage<T, 7, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 8: dyn_stage<T, 8, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 11: dyn_stage<T, 11, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 13: dyn_stage<T, 13, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 16: dyn_stage<T, 16, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      default: break;
+    }
+  }
+  if (d.epi) r2c_epilogue<T>(d, d.P, x, col);
+}
+
+}  // namespace dfft

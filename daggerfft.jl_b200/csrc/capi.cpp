@@ -1,0 +1,104 @@
+// extern "C" entry points of libdfft: argument checks, exception -> status.
+#include <new>
+#include "dfft.h"
+#include "dfft_plan.h"
+
+using dfft::Error;
+
+namespace {
+
+template <class F> int guarded(F&& f) {
+  try {
+    f();
+    return DFFT_SUCCESS;
+  } catch (const Error& e) {
+    dfft::set_error(e.msg);
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    dfft::set_error("host allocation failed");
+    return DFFT_ERROR_OUT_OF_MEMORY;
+  } catch (...) {
+    dfft::set_error("unexpected exception");
+    return DFFT_ERROR_INVALID_VALUE;
+  }
+}
+
+dfft::Plan* impl(dfft_plan p) {
+  if (!p || !p->impl) throw Error{DFFT_ERROR_INVALID_VALUE, "plan is NULL"};
+  return p->impl;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dfft_plan_create(dfft_plan* plan, int ndim, const int64_t* shape, int precision, int transform,
+                     int ndims, const int32_t* dims, const int32_t* r2r_kinds, int64_t irfft_len,
+                     int decomp, int method, unsigned flags) {
+  return guarded([&] {
+    if (!plan) throw Error{DFFT_ERROR_INVALID_VALUE, "plan is NULL"};
+    *plan = nullptr;
+    dfft::Plan* p = dfft::build_plan(ndim, shape, precision, transform, ndims, dims, r2r_kinds,
+                                     irfft_len, decomp, method, flags);
+    *plan = new dfft_plan_s{p};
+  });
+}
+
+int dfft_plan_output_shape(dfft_plan plan, int64_t* shape) {
+  return guarded([&] {
+    dfft::Plan* p = impl(plan);
+    if (!shape) throw Error{DFFT_ERROR_INVALID_VALUE, "shape is NULL"};
+    for (int i = 0; i < p->ndim; ++i) shape[i] = p->out_shape[i];
+  });
+}
+
+int dfft_plan_workspace_bytes(dfft_plan plan, size_t* bytes) {
+  return guarded([&] {
+    dfft::Plan* p = impl(plan);
+    if (!bytes) throw Error{DFFT_ERROR_INVALID_VALUE, "bytes is NULL"};
+    *bytes = p->work_bytes;
+  });
+}
+
+int dfft_plan_launches(dfft_plan plan, int* launches) {
+  return guarded([&] {
+    dfft::Plan* p = impl(plan);
+    if (!launches) throw Error{DFFT_ERROR_INVALID_VALUE, "launches is NULL"};
+    *launches = (int)p->passes.size();
+  });
+}
+
+int dfft_execute(dfft_plan plan, const void* in, void* out, void* stream) {
+  return guarded([&] {
+    dfft::execute_plan(impl(plan), in, out, reinterpret_cast<cudaStream_t>(stream));
+  });
+}
+
+int dfft_plan_destroy(dfft_plan plan) {
+  return guarded([&] {
+    if (!plan) return;
+    delete plan->impl;
+    delete plan;
+  });
+}
+
+const char* dfft_last_error(void) { return dfft::last_error(); }
+
+const char* dfft_status_string(int status) {
+  switch (status) {
+    case DFFT_SUCCESS: return "success";
+    case DFFT_ERROR_INVALID_VALUE: return "invalid value";
+    case DFFT_ERROR_UNKNOWN_TRANSFORM: return "Unknown transform type";
+    case DFFT_ERROR_UNSUPPORTED_SIZE: return "unsupported size";
+    case DFFT_ERROR_CUDA: return "CUDA error";
+    case DFFT_ERROR_OUT_OF_MEMORY: return "out of memory";
+    case DFFT_ERROR_NOT_READY: return "not ready";
+    case DFFT_ERROR_TIMEOUT: return "timeout";
+    case DFFT_ERROR_CANCELLED: return "cancelled";
+    default: return "unknown status";
+  }
+}
+
+const char* dfft_version(void) { return "0.1.0"; }
+
+}  // extern "C"

@@ -1,0 +1,73 @@
+// Host-side declarations shared by the planner, the C ABI and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <memory>
+#include <string>
+#include <vector>
+#include "axis_pass.cuh"
+
+namespace dfft {
+
+// Error reporting: every failing path records a message for dfft_last_error.
+void set_error(const std::string& msg);
+const char* last_error();
+
+struct Error {
+  int status;
+  std::string msg;
+};
+
+// Throws Error{DFFT_ERROR_CUDA, ...} when e != cudaSuccess.
+void cuda_check(cudaError_t e, const char* what);
+
+// A device table owned by the table cache (shared between plans).
+struct DevTable {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int device = -1;
+  ~DevTable();
+};
+
+// Entries exp(-2 pi i (a*k + b) / D) for k = 0..count-1 (exp(+...) if conj),
+// evaluated in long double and rounded to the plan precision.
+std::shared_ptr<DevTable> twiddle_table(int dbl, long long D, long long a, long long b, int count,
+                                        bool conj);
+
+// One kernel launch of a plan.
+enum BufId : int { BUF_IN = 0, BUF_OUT = 1, BUF_WORK = 2 };
+
+struct Pass {
+  PassDesc d{};
+  const void* fn = nullptr;
+  dim3 grid, block;
+  size_t smem = 0;
+  int src = BUF_IN, dst = BUF_OUT;
+  bool is_static = false;
+  std::vector<std::shared_ptr<DevTable>> tables;
+};
+
+// Pass construction.
+struct PassSpec {
+  int dbl = 0;
+  int L = 1;                 // FFT length
+  long long I = 1, O = 1;    // column split
+  int inverse = 0;
+  double scale = 1.0;
+  IoAny in{}, out{};         // pointers filled at execute time
+  bool epi = false;          // R2C half-length post-pass
+  bool fast_io = false;      // plain complex in/out
+};
+
+// Builds a launchable pass; throws Error on unsupported sizes.
+Pass make_pass(const PassSpec& s);
+
+// Launches one pass on `stream` with the given buffers.
+cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream);
+
+// Raise the dynamic shared-memory limit of a kernel on the current device.
+cudaError_t ensure_smem_attr(const void* fn, size_t bytes);
+
+const void* dynamic_kernel(int dbl);
+
+}  // namespace dfft

@@ -1,0 +1,38 @@
+// The plan object behind the opaque dfft_plan handle.
+#pragma once
+#include <vector>
+#include "dfft_internal.h"
+
+namespace dfft {
+
+struct Plan {
+  int device = 0;
+  int ndim = 3;
+  int precision = 0;
+  int transform = 0;
+  int decomp = 0;
+  int method = 0;
+  unsigned flags = 0;
+  std::vector<int> dims;          // 0-based transformed axes
+  int64_t in_shape[3] = {1, 1, 1};
+  int64_t out_shape[3] = {1, 1, 1};
+  size_t in_elem = 0, out_elem = 0;
+  std::vector<Pass> passes;
+  void* work = nullptr;           // plan-owned workspace (C2R over several dims)
+  size_t work_bytes = 0;
+  ~Plan();
+  size_t in_bytes() const;
+  size_t out_bytes() const;
+};
+
+Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, int ndims,
+                 const int32_t* dims, const int32_t* r2r_kinds, int64_t irfft_len, int decomp,
+                 int method, unsigned flags);
+
+void execute_plan(const Plan* p, const void* in, void* out, cudaStream_t stream);
+
+}  // namespace dfft
+
+struct dfft_plan_s {
+  dfft::Plan* impl;
+};

@@ -1,0 +1,267 @@
+// Pass construction: radix plan lookup, launch shape, twiddle tables.
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <unordered_map>
+#include "dfft.h"
+#include "dfft_internal.h"
+#include "static_plans.h"
+
+namespace dfft {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    throw Error{e == cudaErrorMemoryAllocation ? DFFT_ERROR_OUT_OF_MEMORY : DFFT_ERROR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e)};
+  }
+}
+
+// ---------------------------------------------------------------------------
+// twiddle tables
+// ---------------------------------------------------------------------------
+
+DevTable::~DevTable() {
+  if (p) {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != device) cudaSetDevice(device);
+    cudaFree(p);
+    if (cur != device && cur >= 0) cudaSetDevice(cur);
+  }
+}
+
+namespace {
+std::mutex g_tab_mu;
+std::map<std::tuple<int, int, long long, long long, long long, int, bool>, std::weak_ptr<DevTable>>
+    g_tabs;
+}  // namespace
+
+std::shared_ptr<DevTable> twiddle_table(int dbl, long long D, long long a, long long b, int count,
+                                        bool conj) {
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  auto key = std::make_tuple(dev, dbl, D, a, b, count, conj);
+  std::lock_guard<std::mutex> lk(g_tab_mu);
+  auto it = g_tabs.find(key);
+  if (it != g_tabs.end()) {
+    if (auto sp = it->second.lock()) return sp;
+  }
+  const long double two_pi = 2.0L * acosl(-1.0L);
+  const size_t esz = dbl ? 16 : 8;
+  std::vector<unsigned char> host(esz * (size_t)(count > 0 ? count : 1));
+  for (int k = 0; k < count; ++k) {
+    // exact integer reduction of the phase keeps the angle in [0, 2 pi)
+    long long m = ((a * (long long)k + b) % D + D) % D;
+    long double ang = two_pi * (long double)m / (long double)D;
+    long double c = cosl(ang), s = -sinl(ang);
+    if (conj) s = -s;
+    if (dbl) {
+      double v[2] = {(double)c, (double)s};
+      std::memcpy(host.data() + esz * k, v, esz);
+    } else {
+      float v[2] = {(float)c, (float)s};
+      std::memcpy(host.data() + esz * k, v, esz);
+    }
+  }
+  auto t = std::make_shared<DevTable>();
+  t->device = dev;
+  t->bytes = host.size();
+  cuda_check(cudaMalloc(&t->p, t->bytes), "cudaMalloc(twiddles)");
+  cuda_check(cudaMemcpy(t->p, host.data(), t->bytes, cudaMemcpyHostToDevice), "cudaMemcpy(twiddles)");
+  g_tabs[key] = t;
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// static plan lookup
+// ---------------------------------------------------------------------------
+
+namespace {
+std::once_flag g_static_once;
+std::unordered_map<int, const StaticPlan*> g_static[2];
+
+void build_static_index() {
+  for (int dbl = 0; dbl < 2; ++dbl) {
+    const StaticPlanTable* t = dbl ? kTable_f64 : kTable_f32;
+    for (int part = 0; part < kTableParts; ++part) {
+      for (int i = 0; i < *t[part].count; ++i) g_static[dbl][t[part].plans[i].L] = &t[part].plans[i];
+    }
+  }
+}
+
+const StaticPlan* find_static(int dbl, int L) {
+  std::call_once(g_static_once, build_static_index);
+  auto it = g_static[dbl].find(L);
+  return it == g_static[dbl].end() ? nullptr : it->second;
+}
+
+// Radix list for the dynamic kernel: 16/8/4/2 for the power of two, then
+// the odd primes 3, 5, 7, 11, 13.  Empty if L has another prime factor.
+std::vector<int> dynamic_radices(int L) {
+  std::vector<int> r;
+  int n = L;
+  const int odd[] = {13, 11, 7, 5, 3};
+  for (int p : odd) {
+    while (n % p == 0) { r.push_back(p); n /= p; }
+  }
+  int e = 0;
+  while (n % 2 == 0) { ++e; n /= 2; }
+  if (n != 1) return {};
+  while (e >= 4) { r.push_back(16); e -= 4; }
+  if (e == 3) r.push_back(8);
+  if (e == 2) r.push_back(4);
+  if (e == 1) r.push_back(2);
+  if (r.empty()) r.push_back(1);
+  return r;
+}
+
+std::mutex g_attr_mu;
+std::map<std::pair<int, const void*>, size_t> g_attr;
+}  // namespace
+
+cudaError_t ensure_smem_attr(const void* fn, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  auto key = std::make_pair(dev, fn);
+  auto it = g_attr.find(key);
+  if (it != g_attr.end() && it->second >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) g_attr[key] = bytes;
+  return e;
+}
+
+static int swz_host(int k, int esz) { return esz == 8 ? k + (k >> 4) : k + (k >> 3); }
+
+static size_t max_smem_per_block() {
+  static size_t v = 0;
+  if (!v) {
+    int dev = 0, bytes = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+        bytes <= 0)
+      bytes = 227 * 1024;
+    v = (size_t)bytes;
+  }
+  return v;
+}
+
+Pass make_pass(const PassSpec& s) {
+  Pass p;
+  PassDesc& d = p.d;
+  const int L = s.L;
+  if (L < 1) throw Error{DFFT_ERROR_INVALID_VALUE, "transform length must be >= 1"};
+  const StaticPlan* sp = find_static(s.dbl, L);
+  std::vector<int> rad;
+  int P = 0, lb = 1024;
+  if (sp && sp->P <= sp->lb) {
+    rad.assign(sp->radix, sp->radix + sp->nst);
+    P = sp->P;
+    lb = sp->lb;
+    p.fn = s.fast_io ? sp->fast : sp->any;
+    p.is_static = true;
+  } else {
+    rad = dynamic_radices(L);
+    if (rad.empty())
+      throw Error{DFFT_ERROR_UNSUPPORTED_SIZE,
+                  "length " + std::to_string(L) + " has a prime factor above 13"};
+    const int EMAX = 16;
+    P = 1;
+    for (int R : rad) {
+      int B = EMAX / R;
+      int need = (L / R + B - 1) / B;
+      if (need > P) P = need;
+    }
+    lb = 1024;
+    p.fn = dynamic_kernel(s.dbl);
+  }
+  if ((int)rad.size() > kMaxStages)
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "too many stages for length " + std::to_string(L)};
+  d.L = L;
+  d.nst = (int)rad.size();
+  int ns = 1;
+  for (int i = 0; i < d.nst; ++i) {
+    d.radix[i] = rad[i];
+    d.ns[i] = ns;
+    d.tws[i] = L / (ns * rad[i]);
+    ns *= rad[i];
+  }
+  d.P = P;
+  if (P > lb)
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "length " + std::to_string(L) + " exceeds one CTA"};
+  const int esz = s.dbl ? 16 : 8;
+  int ld = swz_host(L - 1, esz) + 1;
+  if ((ld & 1) == 0) ld += 1;
+  d.ld = ld;
+  d.cfast = s.I > 1 ? 1 : 0;
+  const size_t smax = max_smem_per_block();
+  const size_t col_bytes = (size_t)ld * esz;
+  if (col_bytes > smax)
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE,
+                "length " + std::to_string(L) + " does not fit one CTA's shared memory"};
+  int C;
+  if (d.cfast) {
+    // rows of at least 128 bytes for coalesced strided loads, ~256 threads
+    C = s.dbl ? 8 : 16;
+    while (C * P < 256 && C < 64) C *= 2;
+  } else {
+    C = 1;
+    while (C * 2 * P <= 256) C *= 2;
+  }
+  while (C > 1 && (C * P > lb || (size_t)C * col_bytes > smax)) C /= 2;
+  const long long Q = s.I * s.O;
+  if (Q > 0 && C > Q) {
+    // do not launch threads for columns that do not exist
+    int c2 = 1;
+    while (c2 * 2 <= Q) c2 *= 2;
+    if (c2 < C) C = c2;
+  }
+  d.C = C;
+  d.inverse = s.inverse;
+  d.epi = s.epi ? 1 : 0;
+  d.Q = Q;
+  d.I = s.I;
+  d.scale = s.scale;
+  d.in = s.in;
+  d.out = s.out;
+  auto tw = twiddle_table(s.dbl, L, 1, 0, L, false);
+  p.tables.push_back(tw);
+  d.tw = tw->p;
+  if (s.epi) {
+    auto tw2 = twiddle_table(s.dbl, 2LL * L, 1, 0, L + 1, false);
+    p.tables.push_back(tw2);
+    d.tw2 = tw2->p;
+  }
+  const long long nblk = (Q + C - 1) / C;
+  if (nblk > 0x7fffffffLL) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "too many columns for one launch"};
+  p.grid = dim3((unsigned)nblk);
+  p.block = dim3((unsigned)(C * P));
+  p.smem = (size_t)C * col_bytes;
+  return p;
+}
+
+cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream) {
+  if (p.grid.x == 0) return cudaSuccess;
+  cudaError_t e = ensure_smem_attr(p.fn, p.smem);
+  if (e != cudaSuccess) return e;
+  PassDesc d = p.d;
+  d.in.p = in;
+  d.out.p = out;
+  void* args[] = {&d};
+  return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
+}
+
+}  // namespace dfft

@@ -1,0 +1,302 @@
+// Plans: a transform over a column-major 1-3-D array becomes a list of
+// passes (one per transformed axis), executed in the order the reference's
+// stage drivers use (src/fft.jl:650-776, src/fftgpu.jl:497-619).
+#include <algorithm>
+#include <cstring>
+#include "dfft.h"
+#include "dfft_plan.h"
+
+namespace dfft {
+
+namespace {
+
+bool is_c2c(int t) { return t == DFFT_FFT || t == DFFT_IFFT || t == DFFT_FFT_INPLACE || t == DFFT_IFFT_INPLACE; }
+bool is_inverse_c2c(int t) { return t == DFFT_IFFT || t == DFFT_IFFT_INPLACE; }
+bool is_rfft(int t) { return t == DFFT_RFFT || t == DFFT_RFFT_INPLACE; }
+bool is_irfft(int t) { return t == DFFT_IRFFT || t == DFFT_IRFFT_INPLACE; }
+
+// Column split of axis a of a 3-D shape: I = product of the faster dims,
+// O = product of the slower dims.
+void split(const int64_t S[3], int a, long long* I, long long* O) {
+  long long i = 1, o = 1;
+  for (int k = 0; k < a; ++k) i *= S[k];
+  for (int k = a + 1; k < 3; ++k) o *= S[k];
+  *I = i;
+  *O = o;
+}
+
+IoAny io(int kind, long long I, long long extent) {
+  IoAny x{};
+  x.kind = kind;
+  x.si = 1;
+  x.so = I * extent;
+  x.sk = I;
+  return x;
+}
+
+}  // namespace
+
+Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, int ndims,
+                 const int32_t* dims, const int32_t* r2r_kinds, int64_t irfft_len, int decomp,
+                 int method, unsigned flags) {
+  if (ndim < 1 || ndim > 3) throw Error{DFFT_ERROR_INVALID_VALUE, "ndim must be 1, 2 or 3"};
+  if (!shape) throw Error{DFFT_ERROR_INVALID_VALUE, "shape is NULL"};
+  if (precision != DFFT_F32 && precision != DFFT_F64)
+    throw Error{DFFT_ERROR_INVALID_VALUE, "precision must be DFFT_F32 or DFFT_F64"};
+  if (transform < DFFT_FFT || transform > DFFT_R2R)
+    throw Error{DFFT_ERROR_UNKNOWN_TRANSFORM, "Unknown transform type"};
+  if (decomp != DFFT_PENCIL && decomp != DFFT_SLAB)
+    throw Error{DFFT_ERROR_INVALID_VALUE, "decomp must be DFFT_PENCIL or DFFT_SLAB"};
+  if (method != DFFT_PLAIN && method != DFFT_MIXED)
+    throw Error{DFFT_ERROR_INVALID_VALUE, "method must be DFFT_PLAIN or DFFT_MIXED"};
+  if (ndims < 0 || ndims > ndim || (ndims > 0 && !dims))
+    throw Error{DFFT_ERROR_INVALID_VALUE, "dims must list 0..ndim distinct axes"};
+  std::vector<int> ax;
+  for (int i = 0; i < ndims; ++i) {
+    int a = dims[i] - 1;
+    if (a < 0 || a >= ndim) throw Error{DFFT_ERROR_INVALID_VALUE, "dims entry out of range"};
+    if (std::find(ax.begin(), ax.end(), a) != ax.end())
+      throw Error{DFFT_ERROR_INVALID_VALUE, "dims entries must be distinct"};
+    ax.push_back(a);
+  }
+  for (int i = 0; i < ndim; ++i)
+    if (shape[i] < 1) throw Error{DFFT_ERROR_INVALID_VALUE, "shape entries must be >= 1"};
+
+  std::unique_ptr<Plan> P(new Plan());
+  P->ndim = ndim;
+  P->precision = precision;
+  P->transform = transform;
+  P->decomp = decomp;
+  P->method = method;
+  P->flags = flags;
+  P->dims = ax;
+  cuda_check(cudaGetDevice(&P->device), "cudaGetDevice");
+  const int dbl = precision == DFFT_F64 ? 1 : 0;
+  const size_t rsz = dbl ? 8 : 4, csz = 2 * rsz;
+  int64_t S[3] = {1, 1, 1};
+  for (int i = 0; i < ndim; ++i) S[i] = shape[i];
+  for (int i = 0; i < 3; ++i) { P->in_shape[i] = S[i]; P->out_shape[i] = S[i]; }
+  for (int a : ax)
+    if (S[a] > 0x7fffffffLL) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "axis too long"};
+
+  if (method == DFFT_MIXED && !(is_c2c(transform) && !dbl))
+    throw Error{DFFT_ERROR_INVALID_VALUE, "the mixed form supports ComplexF32 FFT/IFFT only"};
+
+  if (is_c2c(transform)) {
+    const bool inv = is_inverse_c2c(transform);
+    P->in_elem = P->out_elem = csz;
+    std::vector<int> order = ax;
+    if (inv) std::reverse(order.begin(), order.end());  // ifft!: dims[3] first
+    int src = BUF_IN;
+    for (int a : order) {
+      PassSpec s;
+      s.dbl = dbl;
+      s.L = (int)S[a];
+      split(S, a, &s.I, &s.O);
+      s.inverse = inv ? 1 : 0;
+      s.scale = inv ? 1.0 / (double)S[a] : 1.0;
+      s.in = io(IO_CPLX, s.I, S[a]);
+      s.out = io(IO_CPLX, s.I, S[a]);
+      s.fast_io = true;
+      Pass p = make_pass(s);
+      p.src = src;
+      p.dst = BUF_OUT;
+      src = BUF_OUT;
+      P->passes.push_back(std::move(p));
+    }
+  } else if (is_rfft(transform)) {
+    if (ax.empty()) throw Error{DFFT_ERROR_INVALID_VALUE, "rfft needs at least one dim"};
+    P->in_elem = rsz;
+    P->out_elem = csz;
+    const int a0 = ax[0];
+    const int64_t n = S[a0];
+    int64_t H[3] = {S[0], S[1], S[2]};
+    H[a0] = n / 2 + 1;
+    for (int i = 0; i < 3; ++i) P->out_shape[i] = H[i];
+    PassSpec s;
+    s.dbl = dbl;
+    split(S, a0, &s.I, &s.O);
+    if (n % 2 == 0) {
+      s.L = (int)(n / 2);
+      s.in = io(IO_REAL_PAIR, s.I, n);
+      s.out = io(IO_CPLX, s.I, H[a0]);
+      s.epi = true;
+    } else {
+      s.L = (int)n;
+      s.in = io(IO_REAL, s.I, n);
+      s.out = io(IO_TRUNC, s.I, H[a0]);
+      s.out.n = (int)(n / 2);
+    }
+    Pass p0 = make_pass(s);
+    p0.src = BUF_IN;
+    p0.dst = BUF_OUT;
+    P->passes.push_back(std::move(p0));
+    for (size_t i = 1; i < ax.size(); ++i) {
+      const int a = ax[i];
+      PassSpec c;
+      c.dbl = dbl;
+      c.L = (int)H[a];
+      split(H, a, &c.I, &c.O);
+      c.in = io(IO_CPLX, c.I, H[a]);
+      c.out = io(IO_CPLX, c.I, H[a]);
+      c.fast_io = true;
+      Pass p = make_pass(c);
+      p.src = BUF_OUT;
+      p.dst = BUF_OUT;
+      P->passes.push_back(std::move(p));
+    }
+  } else if (is_irfft(transform)) {
+    if (ax.empty()) throw Error{DFFT_ERROR_INVALID_VALUE, "irfft needs at least one dim"};
+    const int a0 = ax[0];
+    const int64_t d = irfft_len;
+    if (d < 1 || d / 2 + 1 != S[a0])
+      throw Error{DFFT_ERROR_INVALID_VALUE,
+                  "irfft: the real length d must satisfy d/2+1 == size(F, dims[1])"};
+    P->in_elem = csz;
+    P->out_elem = rsz;
+    int64_t R[3] = {S[0], S[1], S[2]};
+    R[a0] = d;
+    for (int i = 0; i < 3; ++i) P->out_shape[i] = R[i];
+    const bool destroy = (flags & DFFT_FLAG_DESTROY_INPUT) || transform == DFFT_IRFFT_INPLACE;
+    int src = BUF_IN;
+    const int work = destroy ? BUF_IN : BUF_WORK;
+    // inverse C2C along dims[end..2] (reverse stage order), then C2R on dims[1]
+    for (size_t i = ax.size(); i-- > 1;) {
+      const int a = ax[i];
+      PassSpec c;
+      c.dbl = dbl;
+      c.L = (int)S[a];
+      split(S, a, &c.I, &c.O);
+      c.inverse = 1;
+      c.scale = 1.0 / (double)S[a];
+      c.in = io(IO_CPLX, c.I, S[a]);
+      c.out = io(IO_CPLX, c.I, S[a]);
+      c.fast_io = true;
+      Pass p = make_pass(c);
+      p.src = src;
+      p.dst = work;
+      src = work;
+      P->passes.push_back(std::move(p));
+    }
+    if (src == BUF_WORK || (!destroy && ax.size() > 1)) {
+      P->work_bytes = (size_t)(S[0] * S[1] * S[2]) * csz;
+    }
+    PassSpec s;
+    s.dbl = dbl;
+    split(S, a0, &s.I, &s.O);
+    s.inverse = 1;
+    s.scale = 1.0 / (double)d;
+    if (d % 2 == 0) {
+      s.L = (int)(d / 2);
+      s.in = io(IO_HERM_PAIR, s.I, S[a0]);
+      s.in.n = s.L;
+      s.out = io(IO_REAL_PAIR, s.I, d);
+    } else {
+      s.L = (int)d;
+      s.in = io(IO_HERM_FULL, s.I, S[a0]);
+      s.in.n = (int)d;
+      s.out = io(IO_REAL, s.I, d);
+    }
+    Pass p = make_pass(s);
+    if (d % 2 == 0) {
+      auto w = twiddle_table(dbl, d, 1, 0, (int)(d / 2) + 1, false);
+      p.tables.push_back(w);
+      p.d.in.w = w->p;
+    }
+    p.src = src;
+    p.dst = BUF_OUT;
+    P->passes.push_back(std::move(p));
+  } else {  // DFFT_R2R
+    if (!r2r_kinds && !ax.empty()) throw Error{DFFT_ERROR_INVALID_VALUE, "r2r_kinds is NULL"};
+    P->in_elem = P->out_elem = rsz;
+    int src = BUF_IN;
+    for (size_t i = 0; i < ax.size(); ++i) {
+      const int a = ax[i];
+      const int kind = r2r_kinds[i];
+      const int64_t N = S[a];
+      PassSpec s;
+      s.dbl = dbl;
+      split(S, a, &s.I, &s.O);
+      s.in = io(IO_R2R, s.I, N);
+      s.out = io(IO_R2R, s.I, N);
+      s.in.r2r = s.out.r2r = kind;
+      s.in.n = s.out.n = (int)N;
+      std::shared_ptr<DevTable> win, wout;
+      switch (kind) {
+        case DFFT_REDFT10:
+        case DFFT_RODFT10:
+          s.L = (int)N;
+          wout = twiddle_table(dbl, 4 * N, 1, 0, (int)N, false);
+          break;
+        case DFFT_REDFT01:
+        case DFFT_RODFT01:
+          s.L = (int)N;
+          s.inverse = 1;
+          win = twiddle_table(dbl, 4 * N, 1, 0, (int)N, true);
+          break;
+        case DFFT_REDFT11:
+        case DFFT_RODFT11:
+          s.L = (int)(2 * N);
+          win = twiddle_table(dbl, 4 * N, 1, 0, (int)N, false);
+          wout = twiddle_table(dbl, 8 * N, 2, 1, (int)N, false);
+          break;
+        case DFFT_REDFT00:
+          if (N < 2) throw Error{DFFT_ERROR_INVALID_VALUE, "REDFT00 needs n >= 2"};
+          s.L = (int)(2 * (N - 1));
+          break;
+        case DFFT_RODFT00:
+          s.L = (int)(2 * (N + 1));
+          break;
+        case DFFT_DHT:
+          s.L = (int)N;
+          break;
+        default:
+          throw Error{DFFT_ERROR_UNKNOWN_TRANSFORM, "Unknown transform type"};
+      }
+      Pass p = make_pass(s);
+      if (win) { p.tables.push_back(win); p.d.in.w = win->p; }
+      if (wout) { p.tables.push_back(wout); p.d.out.w = wout->p; }
+      p.src = src;
+      p.dst = BUF_OUT;
+      src = BUF_OUT;
+      P->passes.push_back(std::move(p));
+    }
+  }
+  if (P->work_bytes) {
+    cuda_check(cudaMalloc(&P->work, P->work_bytes), "cudaMalloc(workspace)");
+  }
+  return P.release();
+}
+
+Plan::~Plan() {
+  if (work) {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != device) cudaSetDevice(device);
+    cudaFree(work);
+    if (cur != device && cur >= 0) cudaSetDevice(cur);
+  }
+}
+
+size_t Plan::in_bytes() const { return (size_t)(in_shape[0] * in_shape[1] * in_shape[2]) * in_elem; }
+size_t Plan::out_bytes() const { return (size_t)(out_shape[0] * out_shape[1] * out_shape[2]) * out_elem; }
+
+void execute_plan(const Plan* P, const void* in, void* out, cudaStream_t stream) {
+  if (!in || !out) throw Error{DFFT_ERROR_INVALID_VALUE, "in/out is NULL"};
+  int cur = -1;
+  cuda_check(cudaGetDevice(&cur), "cudaGetDevice");
+  if (cur != P->device) cuda_check(cudaSetDevice(P->device), "cudaSetDevice");
+  cudaError_t err = cudaSuccess;
+  if (P->passes.empty()) {
+    if (in != out) err = cudaMemcpyAsync(out, in, P->in_bytes(), cudaMemcpyDeviceToDevice, stream);
+  }
+  for (const Pass& p : P->passes) {
+    if (err != cudaSuccess) break;
+    void* bufs[3] = {const_cast<void*>(in), out, P->work};
+    err = launch_pass(p, bufs[p.src], bufs[p.dst], stream);
+  }
+  if (cur != P->device) cudaSetDevice(cur);
+  cuda_check(err, "kernel launch");
+}
+
+}  // namespace dfft

@@ -1,0 +1,15 @@
+"""dfft: B200-native transform hot path of DaggerFFT.jl (Python host side).
+
+``import dfft`` after putting ``daggerfft.jl_b200`` on ``sys.path``.  The
+compute runs in ``libdfft.so`` (hand-written sm_100a CUDA kernels behind a C
+ABI, see include/dfft.h); this package is the ctypes host layer that mirrors
+the reference's Julia API.
+"""
+from ._lib import ArgumentError, DFFTError, LIB_PATH, lib
+from .api import (DHT, FFT, FFT_, GPU_PLAN_CACHE, HC2R, IFFT, IFFT_, IRFFT, IRFFT_, R2HC, R2R,
+                  R2R_SUPPORTED_KINDS, REDFT00, REDFT01, REDFT10, REDFT11, RFFT, RFFT_, RODFT00,
+                  RODFT01, RODFT10, RODFT11, Decomposition, Pencil, Plan, Slab, Transform,
+                  apply_gpu_fft_, empty_like_layout, fft, fft_, get_or_create_gpu_plan,
+                  gpu_cleanup_plans, gpu_plan_transform, ifft, ifft_, irfft, rfft)
+
+__version__ = "0.1.0"

@@ -1,0 +1,146 @@
+/*
+ * dfft.h -- C ABI of libdfft, the B200 (sm_100a) transform hot path of
+ * DaggerFFT.jl.
+ *
+ * Conventions shared by every entry point
+ *   - Arrays are column-major (Julia order): dim 1 is contiguous.  Shapes
+ *     are given as int64_t[ndim] in that order, ndim in 1..3.
+ *   - dims are 1-based axis numbers, as in Julia.
+ *   - Complex data is interleaved (re, im): ComplexF32 = 2 x float,
+ *     ComplexF64 = 2 x double.
+ *   - All device pointers are caller-owned CUDA device memory on the device
+ *     that was current when the plan was created.  The library owns plans,
+ *     twiddle tables and workspaces; they stay resident until destroyed.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *     Work is enqueued asynchronously; no call synchronises the stream
+ *     unless documented.
+ *   - Every call returns a dfft_status; 0 is success.  dfft_last_error()
+ *     returns a thread-local message describing the last failure.
+ *   - Numerical conventions follow AbstractFFTs/FFTW: forward sign -1,
+ *     unnormalised; inverse transforms scale by 1/prod(n_i); rfft halves the
+ *     FIRST transformed dim to n/2+1; irfft needs the real length d; r2r
+ *     kinds are FFTW's and unnormalised.
+ *   - Threading: a plan may be used by one stream at a time; distinct plans
+ *     may be used concurrently from any thread.
+ */
+#ifndef DFFT_H
+#define DFFT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DFFT_API __attribute__((visibility("default")))
+#else
+#define DFFT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+typedef enum {
+  DFFT_SUCCESS = 0,
+  DFFT_ERROR_INVALID_VALUE = 1,      /* null pointer, bad rank/dims/shape     */
+  DFFT_ERROR_UNKNOWN_TRANSFORM = 2,  /* reference: ArgumentError("Unknown transform type") */
+  DFFT_ERROR_UNSUPPORTED_SIZE = 3,   /* a length this build cannot transform  */
+  DFFT_ERROR_CUDA = 4,               /* a CUDA runtime call failed            */
+  DFFT_ERROR_OUT_OF_MEMORY = 5,      /* device allocation failed / over budget */
+  DFFT_ERROR_NOT_READY = 6,          /* serving: no completed request yet     */
+  DFFT_ERROR_TIMEOUT = 7,            /* a bounded wait gave up                */
+  DFFT_ERROR_CANCELLED = 8           /* serving: request cancelled            */
+} dfft_status;
+
+/* ---- transform tags (src/fft.jl:17-24) -------------------------------- */
+typedef enum {
+  DFFT_FFT = 0,          /* FFT    : out-of-place complex forward           */
+  DFFT_IFFT = 1,         /* IFFT   : out-of-place complex inverse (1/N)      */
+  DFFT_RFFT = 2,         /* RFFT   : real -> half complex                     */
+  DFFT_IRFFT = 3,        /* IRFFT  : half complex -> real, needs real length  */
+  DFFT_FFT_INPLACE = 4,  /* FFT!                                             */
+  DFFT_IFFT_INPLACE = 5, /* IFFT!                                            */
+  DFFT_RFFT_INPLACE = 6, /* RFFT!  (separate output buffer, input preserved)  */
+  DFFT_IRFFT_INPLACE = 7,/* IRFFT! (input may be overwritten as workspace)    */
+  DFFT_R2R = 8           /* R2R((kind,...)) README.md:58-67                   */
+} dfft_transform;
+
+/* element precision of the real or complex data */
+typedef enum { DFFT_F32 = 0, DFFT_F64 = 1 } dfft_precision;
+
+/* decomposition tags (src/fft.jl:13-15) */
+typedef enum { DFFT_PENCIL = 0, DFFT_SLAB = 1 } dfft_decomp;
+
+/* arithmetic form: PLAIN = FP32/FP64 CUDA-core Stockham; MIXED = tensor-core
+ * radix-16/32 stages with FP16 hi+lo split products (ComplexF32 only) */
+typedef enum { DFFT_PLAIN = 0, DFFT_MIXED = 1 } dfft_method;
+
+/* FFTW r2r kinds (fftw_r2r_kind values; src/fft.jl:1-11) */
+enum {
+  DFFT_R2HC = 0, DFFT_HC2R = 1, DFFT_DHT = 2,
+  DFFT_REDFT00 = 3, DFFT_REDFT01 = 4, DFFT_REDFT10 = 5, DFFT_REDFT11 = 6,
+  DFFT_RODFT00 = 7, DFFT_RODFT01 = 8, DFFT_RODFT10 = 9, DFFT_RODFT11 = 10
+};
+
+/* plan flags */
+enum {
+  DFFT_FLAG_DESTROY_INPUT = 1u << 0, /* C2R may use its input as workspace   */
+  DFFT_FLAG_TUNE = 1u << 1,          /* time launch candidates at creation   */
+  DFFT_FLAG_NO_WISDOM = 1u << 2      /* ignore the tuning cache              */
+};
+
+typedef struct dfft_plan_s* dfft_plan;
+
+/*
+ * Plan creation.  Replaces the reference's plan layer:
+ *   plan_transform / get_or_create_plan   (src/fft.jl:126-166)
+ *   gpu_plan_transform / get_or_create_gpu_plan (src/fft.jl: n/a,
+ *   src/fftgpu.jl:85-116)
+ * shape      : INPUT array shape, column-major, ndim in 1..3.  For IRFFT this
+ *              is the half-complex input shape (dims[0] extent d/2+1).
+ * ndims,dims : the transformed axes, 1-based, in the order the stages run
+ *              (Pencil: one stage per entry; Slab: dims[0],dims[1] form the
+ *              2-D slab stage).  Any subset of {1..ndim}.
+ * r2r_kinds  : DFFT_R2R only, one FFTW kind per entry of dims.
+ * irfft_len  : DFFT_IRFFT(_INPLACE) only: the real length d along dims[0].
+ * Unknown `transform` values return DFFT_ERROR_UNKNOWN_TRANSFORM with the
+ * message "Unknown transform type" (src/fft.jl:142, src/fftgpu.jl:103).
+ */
+DFFT_API int dfft_plan_create(dfft_plan* plan, int ndim, const int64_t* shape, int precision,
+                     int transform, int ndims, const int32_t* dims, const int32_t* r2r_kinds,
+                     int64_t irfft_len, int decomp, int method, unsigned flags);
+
+/* Output shape (column-major, ndim entries) of a plan. */
+DFFT_API int dfft_plan_output_shape(dfft_plan plan, int64_t* shape);
+
+/* Device workspace the plan holds (bytes, twiddles excluded). */
+DFFT_API int dfft_plan_workspace_bytes(dfft_plan plan, size_t* bytes);
+
+/* Number of kernel launches one dfft_execute makes. */
+DFFT_API int dfft_plan_launches(dfft_plan plan, int* launches);
+
+/*
+ * Execute: out = T(in).  Replaces apply_fft! / apply_gpu_fft!
+ * (`mul!(out, plan, in)`, src/fft.jl:168-174, src/fftgpu.jl:118-124) and
+ * the per-stage drivers fft!/ifft!/gpu_fft!/gpu_ifft! on one GPU
+ * (src/fft.jl:650-776, src/fftgpu.jl:497-619): every stage and the
+ * redistribution between stages run as strided tile passes inside HBM.
+ * in == out is allowed for C2C and R2R (in-place).
+ */
+DFFT_API int dfft_execute(dfft_plan plan, const void* in, void* out, void* stream);
+
+/* Release a plan (gpu_cleanup_workspace!, src/fftgpu.jl:630-634). */
+DFFT_API int dfft_plan_destroy(dfft_plan plan);
+
+/* Thread-local description of the last error. */
+DFFT_API const char* dfft_last_error(void);
+DFFT_API const char* dfft_status_string(int status);
+
+/* Library version, e.g. "0.1.0". */
+DFFT_API const char* dfft_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DFFT_H */
