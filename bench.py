@@ -171,6 +171,24 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_profile(args):
+    """A short, untimed run for ncu: one warm-up and one measured launch of a
+    single axis pass (forward C2C, ComplexF32) on a column-major array."""
+    import torch
+    import dfft
+    shape = tuple(int(x) for x in args.shape.split(","))
+    torch.cuda.set_device(0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    a = torch.randn(tuple(reversed(shape)), dtype=torch.complex64, device="cuda", generator=g)
+    A = a.permute(*reversed(range(len(shape))))
+    B = dfft.empty_like_layout(A.shape, A.dtype, A)
+    p = dfft.gpu_plan_transform(dfft.FFT(), A, (args.profile,), method=args.method)
+    for _ in range(2):
+        p.execute(A, B)
+    torch.cuda.synchronize()
+    print(f"profile: dim {args.profile} of {shape}, {p.launches} launch(es) per call, 2 calls")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -179,7 +197,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--method", default="plain", choices=["plain", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", type=int, default=0,
+                    help="profiling mode: run 2 launches of the pass along this dim (1-3) and exit")
+    ap.add_argument("--shape", default="512,512,512", help="profiling mode: ComplexF32 array shape")
     args = ap.parse_args()
+    if args.profile:
+        run_profile(args)
+        return
     args.warmup = max(args.warmup, 3)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -245,17 +245,34 @@ __device__ __forceinline__ void store_elem(const IoAny& io, long long b, int k,
 // Stage body.
 // ---------------------------------------------------------------------------
 
-// BMAX: upper bound on butterflies per thread; in the static kernel it is
+// Shared-memory view of one column.  PadCol: column-major with one pad
+// element per 128 bytes (direct-load kernels); StrideCol: the [k][c] layout a
+// TMA tile box lands in (c fastest), conflict-free for the cfast mapping.
+template <typename V> struct PadCol {
+  V* p;
+  __device__ __forceinline__ V ld(int k) const { return p[swz<V>(k)]; }
+  __device__ __forceinline__ void st(int k, V v) const { p[swz<V>(k)] = v; }
+};
+template <typename V> struct StrideCol {
+  V* p;
+  int s;
+  __device__ __forceinline__ V ld(int k) const { return p[k * s]; }
+  __device__ __forceinline__ void st(int k, V v) const { p[k * s] = v; }
+};
+
+// BMAX: upper bound on butterflies per thread; in the static kernels it is
 // exactly ceil((L/R)/P), in the dynamic kernel EMAX/R.
-template <typename T, int R, int BMAX, bool FAST_IO>
+// SMEM_IO: the first stage reads and the last stage writes the shared tile
+// (TMA kernels) instead of global memory.
+template <typename T, int R, int BMAX, bool FAST_IO, bool SMEM_IO, class COL>
 __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int Ns, int ts,
-                                           bool first, bool last, int t,
-                                           typename cvec<T>::type* col,
+                                           bool first, bool last, int t, const COL& col,
                                            const typename cvec<T>::type* tw,
                                            long long ib, long long ob, bool cv) {
   typedef typename cvec<T>::type V;
   const int Lr = L / R;
-  const bool to_global = last && !d.epi;
+  const bool to_global = !SMEM_IO && last && !d.epi;
+  const bool from_global = !SMEM_IO && first;
   V v[BMAX][R];
 #pragma unroll
   for (int b = 0; b < BMAX; ++b) {
@@ -264,7 +281,7 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const int k = j + r * Lr;
-        if (first) {
+        if (from_global) {
           V x;
           if (!cv) x = mk<V>((T)0, (T)0);
           else if (FAST_IO) x = reinterpret_cast<const V*>(d.in.p)[ib + k * d.in.sk];
@@ -272,12 +289,14 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
           if (d.inverse) x.y = -x.y;
           v[b][r] = x;
         } else {
-          v[b][r] = col[swz<V>(k)];
+          V x = col.ld(k);
+          if (SMEM_IO && first && d.inverse) x.y = -x.y;
+          v[b][r] = x;
         }
       }
     }
   }
-  if (!first) __syncthreads();
+  if (!from_global) __syncthreads();
 #pragma unroll
   for (int b = 0; b < BMAX; ++b) {
     const int j = t + b * P;
@@ -299,8 +318,12 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
             if (FAST_IO) reinterpret_cast<V*>(d.out.p)[ob + k * d.out.sk] = cscale(y, (T)d.scale);
             else store_elem<T>(d.out, ob, k, y, (T)d.scale);
           }
+        } else if (SMEM_IO && last) {
+          V y = v[b][r];
+          if (d.inverse) y.y = -y.y;
+          col.st(k, cscale(y, (T)d.scale));
         } else {
-          col[swz<V>(k)] = v[b][r];
+          col.st(k, v[b][r]);
         }
       }
     }
@@ -351,17 +374,18 @@ __device__ __forceinline__ void r2c_epilogue(const PassDesc& d, int P, const Col
 // Static-plan kernel.
 // ---------------------------------------------------------------------------
 
-template <typename T, int L, int P, bool FAST_IO, int NS, int S, int R, int... Rest>
-__device__ __forceinline__ void static_stages(const PassDesc& d, int t, typename cvec<T>::type* col,
+template <typename T, int L, int P, bool FAST_IO, bool SMEM_IO, int NS, int S, class COL, int R,
+          int... Rest>
+__device__ __forceinline__ void static_stages(const PassDesc& d, int t, const COL& col,
                                               const typename cvec<T>::type* tw, long long ib,
                                               long long ob, bool cv) {
   constexpr int Lr = L / R;
   constexpr int BM = (Lr + P - 1) / P;
   constexpr int TS = L / (NS * R);
-  stage_body<T, R, BM, FAST_IO>(d, L, P, NS, TS, S == 0, sizeof...(Rest) == 0, t, col, tw, ib, ob,
-                                cv);
+  stage_body<T, R, BM, FAST_IO, SMEM_IO>(d, L, P, NS, TS, S == 0, sizeof...(Rest) == 0, t, col, tw,
+                                         ib, ob, cv);
   if constexpr (sizeof...(Rest) > 0)
-    static_stages<T, L, P, FAST_IO, NS * R, S + 1, Rest...>(d, t, col, tw, ib, ob, cv);
+    static_stages<T, L, P, FAST_IO, SMEM_IO, NS * R, S + 1, COL, Rest...>(d, t, col, tw, ib, ob, cv);
 }
 
 template <typename T, bool FAST_IO, int LB, int L, int P, int... Rs>
@@ -370,10 +394,10 @@ __global__ void __launch_bounds__(LB) axis_pass_static(const PassDesc d) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* sm = reinterpret_cast<V*>(smem_raw);
   const ColCtx x = col_ctx(d, P);
-  V* col = sm + x.c * d.ld;
+  const PadCol<V> col{sm + x.c * d.ld};
   const V* tw = reinterpret_cast<const V*>(d.tw);
-  static_stages<T, L, P, FAST_IO, 1, 0, Rs...>(d, x.t, col, tw, x.ib, x.ob, x.cv);
-  if (!FAST_IO && d.epi) r2c_epilogue<T>(d, P, x, col);
+  static_stages<T, L, P, FAST_IO, false, 1, 0, PadCol<V>, Rs...>(d, x.t, col, tw, x.ib, x.ob, x.cv);
+  if (!FAST_IO && d.epi) r2c_epilogue<T>(d, P, x, col.p);
 }
 
 // ---------------------------------------------------------------------------
@@ -384,8 +408,9 @@ template <typename T, int R, int EMAX>
 __device__ __noinline__ void dyn_stage(const PassDesc& d, int s, int t, typename cvec<T>::type* col,
                                        const typename cvec<T>::type* tw, long long ib, long long ob,
                                        bool cv) {
-  stage_body<T, R, EMAX / R, false>(d, d.L, d.P, d.ns[s], d.tws[s], s == 0, s == d.nst - 1, t, col,
-                                    tw, ib, ob, cv);
+  const PadCol<typename cvec<T>::type> c{col};
+  stage_body<T, R, EMAX / R, false, false>(d, d.L, d.P, d.ns[s], d.tws[s], s == 0, s == d.nst - 1,
+                                           t, c, tw, ib, ob, cv);
 }
 
 template <typename T, int EMAX>

@@ -82,6 +82,17 @@ int dfft_plan_destroy(dfft_plan plan) {
   });
 }
 
+int dfft_device_error(int* code) {
+  return guarded([&] {
+    if (!code) throw Error{DFFT_ERROR_INVALID_VALUE, "code is NULL"};
+    int* w = dfft::device_error_word();
+    int v = 0;
+    dfft::cuda_check(cudaMemcpy(&v, w, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(error word)");
+    dfft::cuda_check(cudaMemset(w, 0, sizeof(int)), "cudaMemset(error word)");
+    *code = v;
+  });
+}
+
 const char* dfft_last_error(void) { return dfft::last_error(); }
 
 const char* dfft_status_string(int status) {

@@ -5,7 +5,7 @@
 #include <memory>
 #include <string>
 #include <vector>
-#include "axis_pass.cuh"
+#include "tma_pass.cuh"
 
 namespace dfft {
 
@@ -44,8 +44,15 @@ struct Pass {
   size_t smem = 0;
   int src = BUF_IN, dst = BUF_OUT;
   bool is_static = false;
+  // TMA-pipelined strided pass: tensor {I*xscale, L, O} of 8-byte elements
+  bool tma = false;
+  TmaGeom geom{};
+  long long tI = 0, tL = 0, tO = 0;
   std::vector<std::shared_ptr<DevTable>> tables;
 };
+
+// Device error word of the current device (bounded waits that expire set it).
+int* device_error_word();
 
 // Pass construction.
 struct PassSpec {

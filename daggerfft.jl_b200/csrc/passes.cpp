@@ -5,6 +5,7 @@
 #include <mutex>
 #include <tuple>
 #include <unordered_map>
+#include <cuda.h>
 #include "dfft.h"
 #include "dfft_internal.h"
 #include "static_plans.h"
@@ -144,6 +145,75 @@ cudaError_t ensure_smem_attr(const void* fn, size_t bytes) {
   return e;
 }
 
+// ---------------------------------------------------------------------------
+// device error word and TMA descriptors
+// ---------------------------------------------------------------------------
+
+namespace {
+std::mutex g_err_mu;
+std::map<int, int*> g_err_words;
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn g_encode = nullptr;
+std::once_flag g_encode_once;
+
+void load_encode() {
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+      q == cudaDriverEntryPointSuccess)
+    g_encode = reinterpret_cast<EncodeTiledFn>(fn);
+}
+}  // namespace
+
+int* device_error_word() {
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  auto it = g_err_words.find(dev);
+  if (it != g_err_words.end()) return it->second;
+  int* w = nullptr;
+  cuda_check(cudaMalloc(&w, sizeof(int)), "cudaMalloc(error word)");
+  cuda_check(cudaMemset(w, 0, sizeof(int)), "cudaMemset(error word)");
+  g_err_words[dev] = w;
+  return w;
+}
+
+static cudaError_t encode_map(CUtensorMap* m, void* base, const Pass& p) {
+  std::call_once(g_encode_once, load_encode);
+  if (!g_encode) return cudaErrorNotSupported;
+  const cuuint64_t esz = 8;
+  const cuuint64_t xs = (cuuint64_t)p.geom.xscale;
+  cuuint64_t dims[3] = {(cuuint64_t)p.tI * xs, (cuuint64_t)p.tL, (cuuint64_t)p.tO};
+  cuuint64_t strides[2] = {(cuuint64_t)p.tI * xs * esz, (cuuint64_t)p.tI * xs * esz * (cuuint64_t)p.tL};
+  cuuint32_t box[3] = {(cuuint32_t)(p.geom.C * p.geom.xscale), (cuuint32_t)p.geom.lb, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+static int sm_count() {
+  static int v = 0;
+  if (!v) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+  }
+  return v;
+}
+
+// Rows per TMA box: the largest divisor of L not above 256.
+static int box_rows(int L) {
+  for (int r = L < 256 ? L : 256; r >= 1; --r)
+    if (L % r == 0) return r;
+  return 1;
+}
+
 static int swz_host(int k, int esz) { return esz == 8 ? k + (k >> 4) : k + (k >> 3); }
 
 static size_t max_smem_per_block() {
@@ -229,6 +299,32 @@ Pass make_pass(const PassSpec& s) {
     while (c2 * 2 <= Q) c2 *= 2;
     if (c2 < C) C = c2;
   }
+  // TMA-pipelined variant for strided C2C passes (8-byte TMA elements need
+  // 16-byte row strides; three tile buffers must fit in shared memory)
+  if (p.is_static && sp->tma && s.fast_io && s.I > 1 && (s.I * esz) % 16 == 0 && s.I < (1LL << 31) &&
+      s.O < (1LL << 31) && (s.I + C - 1) / C < (1LL << 31)) {
+    int Ct = s.dbl ? 8 : 16;
+    while (Ct * P < 256 && Ct < 64 && (size_t)kTmaBufs * 2 * Ct * L * esz + 128 <= smax) Ct *= 2;
+    const int tlb = sp->tma_lb;
+    while (Ct > 4 && (Ct * P > tlb || (size_t)kTmaBufs * Ct * L * esz + 128 > smax)) Ct /= 2;
+    if (Ct * P <= tlb && (size_t)kTmaBufs * Ct * L * esz + 128 <= smax) {
+      p.tma = true;
+      p.fn = sp->tma;
+      p.tI = s.I;
+      p.tL = L;
+      p.tO = s.O;
+      TmaGeom& g = p.geom;
+      g.C = Ct;
+      g.tiles_i = (int)((s.I + Ct - 1) / Ct);
+      g.ntiles = (long long)g.tiles_i * s.O;
+      g.lb = box_rows(L);
+      g.nlb = L / g.lb;
+      g.xscale = s.dbl ? 2 : 1;
+      g.tile_bytes = (unsigned)((size_t)Ct * L * esz);
+      g.err = device_error_word();
+      C = Ct;
+    }
+  }
   d.C = C;
   d.inverse = s.inverse;
   d.epi = s.epi ? 1 : 0;
@@ -245,6 +341,19 @@ Pass make_pass(const PassSpec& s) {
     p.tables.push_back(tw2);
     d.tw2 = tw2->p;
   }
+  if (p.tma) {
+    p.block = dim3((unsigned)(C * P));
+    p.smem = 128 + (size_t)kTmaBufs * C * L * esz;
+    cuda_check(ensure_smem_attr(p.fn, p.smem), "cudaFuncSetAttribute(tma)");
+    int occ = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p.fn, (int)p.block.x, p.smem),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (occ < 1) occ = 1;
+    long long nb = (long long)sm_count() * occ;
+    if (nb > p.geom.ntiles) nb = p.geom.ntiles;
+    p.grid = dim3((unsigned)(nb > 0 ? nb : 1));
+    return p;
+  }
   const long long nblk = (Q + C - 1) / C;
   if (nblk > 0x7fffffffLL) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "too many columns for one launch"};
   p.grid = dim3((unsigned)nblk);
@@ -260,6 +369,18 @@ cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream)
   PassDesc d = p.d;
   d.in.p = in;
   d.out.p = out;
+  if (p.tma) {
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
+      return cudaErrorMisalignedAddress;
+    CUtensorMap tin, tout;
+    e = encode_map(&tin, in, p);
+    if (e != cudaSuccess) return e;
+    e = encode_map(&tout, out, p);
+    if (e != cudaSuccess) return e;
+    TmaGeom g = p.geom;
+    void* args[] = {&d, &tin, &tout, &g};
+    return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
+  }
   void* args[] = {&d};
   return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
 }

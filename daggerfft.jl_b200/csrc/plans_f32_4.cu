@@ -5,30 +5,43 @@ template __global__ void axis_pass_static<float,true,1024,5,1,5>(const PassDesc)
 template __global__ void axis_pass_static<float,false,1024,5,1,5>(const PassDesc);
 template __global__ void axis_pass_static<float,true,1024,15,1,15>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,15,1,15>(const PassDesc);
+template __global__ void axis_pass_tma<float,1024,15,1,15>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,27,9,3,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,27,9,3,3,3>(const PassDesc);
+template __global__ void axis_pass_tma<float,1024,27,9,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,48,6,6,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,48,6,6,8>(const PassDesc);
+template __global__ void axis_pass_tma<float,1024,48,6,6,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,75,5,15,5>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,75,5,15,5>(const PassDesc);
+template __global__ void axis_pass_tma<float,1024,75,5,15,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,108,18,6,6,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,108,18,6,6,3>(const PassDesc);
+template __global__ void axis_pass_tma<float,1024,108,18,6,6,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,512,150,10,15,10>(const PassDesc);
 template __global__ void axis_pass_static<float,false,512,150,10,15,10>(const PassDesc);
+template __global__ void axis_pass_tma<float,512,150,10,15,10>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,216,36,6,6,6>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,216,36,6,6,6>(const PassDesc);
+template __global__ void axis_pass_tma<float,1024,216,36,6,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,512,270,18,15,6,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,512,270,18,15,6,3>(const PassDesc);
+template __global__ void axis_pass_tma<float,512,270,18,15,6,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,375,25,15,5,5>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,375,25,15,5,5>(const PassDesc);
+template __global__ void axis_pass_tma<float,1024,375,25,15,5,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,480,48,10,6,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,480,48,10,6,8>(const PassDesc);
+template __global__ void axis_pass_tma<float,1024,480,48,10,6,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,600,60,10,10,6>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,600,60,10,10,6>(const PassDesc);
+template __global__ void axis_pass_tma<float,1024,600,60,10,10,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,729,243,3,3,3,3,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,729,243,3,3,3,3,3,3>(const PassDesc);
+template __global__ void axis_pass_tma<float,1024,729,243,3,3,3,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,512,900,60,15,10,6>(const PassDesc);
 template __global__ void axis_pass_static<float,false,512,900,60,15,10,6>(const PassDesc);
+template __global__ void axis_pass_tma<float,512,900,60,15,10,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,1125,75,15,15,5>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,1125,75,15,15,5>(const PassDesc);
 template __global__ void axis_pass_static<float,true,1024,1296,216,6,6,6,6>(const PassDesc);
@@ -50,29 +63,29 @@ template __global__ void axis_pass_static<float,false,1024,4096,256,16,16,16>(co
 extern const StaticPlan kPlans_f32_4[];
 extern const int kPlansCount_f32_4;
 const StaticPlan kPlans_f32_4[] = {
-  {5, 1, 1, {5}, 1024, (const void*)&axis_pass_static<float,true,1024,5,1,5>, (const void*)&axis_pass_static<float,false,1024,5,1,5>},
-  {15, 1, 1, {15}, 1024, (const void*)&axis_pass_static<float,true,1024,15,1,15>, (const void*)&axis_pass_static<float,false,1024,15,1,15>},
-  {27, 9, 3, {3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,27,9,3,3,3>, (const void*)&axis_pass_static<float,false,1024,27,9,3,3,3>},
-  {48, 6, 2, {6,8}, 1024, (const void*)&axis_pass_static<float,true,1024,48,6,6,8>, (const void*)&axis_pass_static<float,false,1024,48,6,6,8>},
-  {75, 5, 2, {15,5}, 1024, (const void*)&axis_pass_static<float,true,1024,75,5,15,5>, (const void*)&axis_pass_static<float,false,1024,75,5,15,5>},
-  {108, 18, 3, {6,6,3}, 1024, (const void*)&axis_pass_static<float,true,1024,108,18,6,6,3>, (const void*)&axis_pass_static<float,false,1024,108,18,6,6,3>},
-  {150, 10, 2, {15,10}, 512, (const void*)&axis_pass_static<float,true,512,150,10,15,10>, (const void*)&axis_pass_static<float,false,512,150,10,15,10>},
-  {216, 36, 3, {6,6,6}, 1024, (const void*)&axis_pass_static<float,true,1024,216,36,6,6,6>, (const void*)&axis_pass_static<float,false,1024,216,36,6,6,6>},
-  {270, 18, 3, {15,6,3}, 512, (const void*)&axis_pass_static<float,true,512,270,18,15,6,3>, (const void*)&axis_pass_static<float,false,512,270,18,15,6,3>},
-  {375, 25, 3, {15,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,375,25,15,5,5>, (const void*)&axis_pass_static<float,false,1024,375,25,15,5,5>},
-  {480, 48, 3, {10,6,8}, 1024, (const void*)&axis_pass_static<float,true,1024,480,48,10,6,8>, (const void*)&axis_pass_static<float,false,1024,480,48,10,6,8>},
-  {600, 60, 3, {10,10,6}, 1024, (const void*)&axis_pass_static<float,true,1024,600,60,10,10,6>, (const void*)&axis_pass_static<float,false,1024,600,60,10,10,6>},
-  {729, 243, 6, {3,3,3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,729,243,3,3,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,729,243,3,3,3,3,3,3>},
-  {900, 60, 3, {15,10,6}, 512, (const void*)&axis_pass_static<float,true,512,900,60,15,10,6>, (const void*)&axis_pass_static<float,false,512,900,60,15,10,6>},
-  {1125, 75, 3, {15,15,5}, 1024, (const void*)&axis_pass_static<float,true,1024,1125,75,15,15,5>, (const void*)&axis_pass_static<float,false,1024,1125,75,15,15,5>},
-  {1296, 216, 4, {6,6,6,6}, 1024, (const void*)&axis_pass_static<float,true,1024,1296,216,6,6,6,6>, (const void*)&axis_pass_static<float,false,1024,1296,216,6,6,6,6>},
-  {1600, 100, 3, {10,10,16}, 512, (const void*)&axis_pass_static<float,true,512,1600,100,10,10,16>, (const void*)&axis_pass_static<float,false,512,1600,100,10,10,16>},
-  {1944, 324, 5, {6,6,6,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,1944,324,6,6,6,3,3>, (const void*)&axis_pass_static<float,false,1024,1944,324,6,6,6,3,3>},
-  {2250, 150, 3, {15,15,10}, 512, (const void*)&axis_pass_static<float,true,512,2250,150,15,15,10>, (const void*)&axis_pass_static<float,false,512,2250,150,15,15,10>},
-  {2592, 216, 4, {12,6,6,6}, 1024, (const void*)&axis_pass_static<float,true,1024,2592,216,12,6,6,6>, (const void*)&axis_pass_static<float,false,1024,2592,216,12,6,6,6>},
-  {3125, 625, 5, {5,5,5,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,3125,625,5,5,5,5,5>, (const void*)&axis_pass_static<float,false,1024,3125,625,5,5,5,5,5>},
-  {3645, 243, 6, {15,3,3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,3645,243,15,3,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,3645,243,15,3,3,3,3,3>},
-  {4096, 256, 3, {16,16,16}, 1024, (const void*)&axis_pass_static<float,true,1024,4096,256,16,16,16>, (const void*)&axis_pass_static<float,false,1024,4096,256,16,16,16>},
+  {5, 1, 1, {5}, 1024, (const void*)&axis_pass_static<float,true,1024,5,1,5>, (const void*)&axis_pass_static<float,false,1024,5,1,5>, nullptr, 1024},
+  {15, 1, 1, {15}, 1024, (const void*)&axis_pass_static<float,true,1024,15,1,15>, (const void*)&axis_pass_static<float,false,1024,15,1,15>, (const void*)&axis_pass_tma<float,1024,15,1,15>, 1024},
+  {27, 9, 3, {3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,27,9,3,3,3>, (const void*)&axis_pass_static<float,false,1024,27,9,3,3,3>, (const void*)&axis_pass_tma<float,1024,27,9,3,3,3>, 1024},
+  {48, 6, 2, {6,8}, 1024, (const void*)&axis_pass_static<float,true,1024,48,6,6,8>, (const void*)&axis_pass_static<float,false,1024,48,6,6,8>, (const void*)&axis_pass_tma<float,1024,48,6,6,8>, 1024},
+  {75, 5, 2, {15,5}, 1024, (const void*)&axis_pass_static<float,true,1024,75,5,15,5>, (const void*)&axis_pass_static<float,false,1024,75,5,15,5>, (const void*)&axis_pass_tma<float,1024,75,5,15,5>, 1024},
+  {108, 18, 3, {6,6,3}, 1024, (const void*)&axis_pass_static<float,true,1024,108,18,6,6,3>, (const void*)&axis_pass_static<float,false,1024,108,18,6,6,3>, (const void*)&axis_pass_tma<float,1024,108,18,6,6,3>, 1024},
+  {150, 10, 2, {15,10}, 512, (const void*)&axis_pass_static<float,true,512,150,10,15,10>, (const void*)&axis_pass_static<float,false,512,150,10,15,10>, (const void*)&axis_pass_tma<float,512,150,10,15,10>, 512},
+  {216, 36, 3, {6,6,6}, 1024, (const void*)&axis_pass_static<float,true,1024,216,36,6,6,6>, (const void*)&axis_pass_static<float,false,1024,216,36,6,6,6>, (const void*)&axis_pass_tma<float,1024,216,36,6,6,6>, 1024},
+  {270, 18, 3, {15,6,3}, 512, (const void*)&axis_pass_static<float,true,512,270,18,15,6,3>, (const void*)&axis_pass_static<float,false,512,270,18,15,6,3>, (const void*)&axis_pass_tma<float,512,270,18,15,6,3>, 512},
+  {375, 25, 3, {15,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,375,25,15,5,5>, (const void*)&axis_pass_static<float,false,1024,375,25,15,5,5>, (const void*)&axis_pass_tma<float,1024,375,25,15,5,5>, 1024},
+  {480, 48, 3, {10,6,8}, 1024, (const void*)&axis_pass_static<float,true,1024,480,48,10,6,8>, (const void*)&axis_pass_static<float,false,1024,480,48,10,6,8>, (const void*)&axis_pass_tma<float,1024,480,48,10,6,8>, 1024},
+  {600, 60, 3, {10,10,6}, 1024, (const void*)&axis_pass_static<float,true,1024,600,60,10,10,6>, (const void*)&axis_pass_static<float,false,1024,600,60,10,10,6>, (const void*)&axis_pass_tma<float,1024,600,60,10,10,6>, 1024},
+  {729, 243, 6, {3,3,3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,729,243,3,3,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,729,243,3,3,3,3,3,3>, (const void*)&axis_pass_tma<float,1024,729,243,3,3,3,3,3,3>, 1024},
+  {900, 60, 3, {15,10,6}, 512, (const void*)&axis_pass_static<float,true,512,900,60,15,10,6>, (const void*)&axis_pass_static<float,false,512,900,60,15,10,6>, (const void*)&axis_pass_tma<float,512,900,60,15,10,6>, 512},
+  {1125, 75, 3, {15,15,5}, 1024, (const void*)&axis_pass_static<float,true,1024,1125,75,15,15,5>, (const void*)&axis_pass_static<float,false,1024,1125,75,15,15,5>, nullptr, 1024},
+  {1296, 216, 4, {6,6,6,6}, 1024, (const void*)&axis_pass_static<float,true,1024,1296,216,6,6,6,6>, (const void*)&axis_pass_static<float,false,1024,1296,216,6,6,6,6>, nullptr, 1024},
+  {1600, 100, 3, {10,10,16}, 512, (const void*)&axis_pass_static<float,true,512,1600,100,10,10,16>, (const void*)&axis_pass_static<float,false,512,1600,100,10,10,16>, nullptr, 512},
+  {1944, 324, 5, {6,6,6,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,1944,324,6,6,6,3,3>, (const void*)&axis_pass_static<float,false,1024,1944,324,6,6,6,3,3>, nullptr, 1024},
+  {2250, 150, 3, {15,15,10}, 512, (const void*)&axis_pass_static<float,true,512,2250,150,15,15,10>, (const void*)&axis_pass_static<float,false,512,2250,150,15,15,10>, nullptr, 512},
+  {2592, 216, 4, {12,6,6,6}, 1024, (const void*)&axis_pass_static<float,true,1024,2592,216,12,6,6,6>, (const void*)&axis_pass_static<float,false,1024,2592,216,12,6,6,6>, nullptr, 1024},
+  {3125, 625, 5, {5,5,5,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,3125,625,5,5,5,5,5>, (const void*)&axis_pass_static<float,false,1024,3125,625,5,5,5,5,5>, nullptr, 1024},
+  {3645, 243, 6, {15,3,3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,3645,243,15,3,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,3645,243,15,3,3,3,3,3>, nullptr, 1024},
+  {4096, 256, 3, {16,16,16}, 1024, (const void*)&axis_pass_static<float,true,1024,4096,256,16,16,16>, (const void*)&axis_pass_static<float,false,1024,4096,256,16,16,16>, nullptr, 1024},
 };
 const int kPlansCount_f32_4 = 23;
 }  // namespace dfft

@@ -1,6 +1,6 @@
 // Table of the precompiled static-plan kernels (generated by gen_plans.py).
 #pragma once
-#include "axis_pass.cuh"
+#include "tma_pass.cuh"
 
 namespace dfft {
 
@@ -12,6 +12,8 @@ struct StaticPlan {
   int lb;             // __launch_bounds__ of the kernels (max threads per CTA)
   const void* fast;   // axis_pass_static<T, true, ...>: complex in, complex out
   const void* any;    // axis_pass_static<T, false, ...>: any IoKind, R2C post-pass
+  const void* tma;    // axis_pass_tma<T, ...>: strided C2C, TMA-pipelined (or null)
+  int tma_lb;         // __launch_bounds__ of the TMA kernel
 };
 
 struct StaticPlanTable {

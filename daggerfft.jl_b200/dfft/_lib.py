@@ -80,6 +80,8 @@ def lib():
     L.dfft_execute.restype = c_int
     L.dfft_plan_destroy.argtypes = [c_void_p]
     L.dfft_plan_destroy.restype = c_int
+    L.dfft_device_error.argtypes = [ctypes.POINTER(c_int)]
+    L.dfft_device_error.restype = c_int
     L.dfft_last_error.argtypes = []
     L.dfft_last_error.restype = c_char_p
     L.dfft_status_string.argtypes = [c_int]
@@ -108,3 +110,10 @@ def i64_array(vals):
 
 def i32_array(vals):
     return (ctypes.c_int32 * max(1, len(vals)))(*[int(v) for v in vals])
+
+
+def device_error():
+    """Reads and clears the device error word (0 = no kernel gave up a wait)."""
+    v = ctypes.c_int()
+    check(lib().dfft_device_error(ctypes.byref(v)))
+    return v.value

@@ -132,6 +132,14 @@ DFFT_API int dfft_execute(dfft_plan plan, const void* in, void* out, void* strea
 /* Release a plan (gpu_cleanup_workspace!, src/fftgpu.jl:630-634). */
 DFFT_API int dfft_plan_destroy(dfft_plan plan);
 
+/*
+ * Reads and clears the device error word of the current device.  Kernels
+ * whose bounded waits expire (TMA tile pipeline) record a non-zero code there
+ * instead of hanging: 1 = a tile load did not complete in time.  Synchronises
+ * the device.
+ */
+DFFT_API int dfft_device_error(int* code);
+
 /* Thread-local description of the last error. */
 DFFT_API const char* dfft_last_error(void);
 DFFT_API const char* dfft_status_string(int status);
