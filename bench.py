@@ -182,7 +182,8 @@ def run_profile(args):
     a = torch.randn(tuple(reversed(shape)), dtype=torch.complex64, device="cuda", generator=g)
     A = a.permute(*reversed(range(len(shape))))
     B = dfft.empty_like_layout(A.shape, A.dtype, A)
-    p = dfft.gpu_plan_transform(dfft.FFT(), A, (args.profile,), method=args.method)
+    p = dfft.gpu_plan_transform(dfft.FFT(), A, (args.profile,), method=args.method,
+                                flags=0 if args.no_tune else dfft.FLAG_TUNE)
     for _ in range(2):
         p.execute(A, B)
     torch.cuda.synchronize()
@@ -197,6 +198,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--method", default="plain", choices=["plain", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="heuristic launch shapes, no autotuning")
     ap.add_argument("--profile", type=int, default=0,
                     help="profiling mode: run 2 launches of the pass along this dim (1-3) and exit")
     ap.add_argument("--shape", default="512,512,512", help="profiling mode: ComplexF32 array shape")
@@ -234,8 +236,11 @@ def main():
     Bd = dfft.empty_like_layout(Ad.shape, Ad.dtype, Ad)
     Cd = dfft.empty_like_layout(Ad.shape, Ad.dtype, Ad)
     decomp = dfft.Slab()
-    pf = dfft.get_or_create_gpu_plan(dfft.FFT(), Ad, (1, 2, 3), decomp=decomp, method=args.method)
-    pi = dfft.get_or_create_gpu_plan(dfft.IFFT(), Bd, (1, 2, 3), decomp=decomp, method=args.method)
+    flags = 0 if args.no_tune else dfft.FLAG_TUNE
+    pf = dfft.get_or_create_gpu_plan(dfft.FFT(), Ad, (1, 2, 3), decomp=decomp, method=args.method,
+                                     flags=flags)
+    pi = dfft.get_or_create_gpu_plan(dfft.IFFT(), Bd, (1, 2, 3), decomp=decomp, method=args.method,
+                                     flags=flags)
     launches_per_step = pf.launches + pi.launches
 
     def step():
@@ -285,7 +290,8 @@ def main():
     # per-axis kernels timed alone (roofline of the dominant kernel)
     per_axis = {}
     for ax in (1, 2, 3):
-        p = dfft.gpu_plan_transform(dfft.FFT(), Ad, (ax,), decomp=decomp, method=args.method)
+        p = dfft.gpu_plan_transform(dfft.FFT(), Ad, (ax,), decomp=decomp, method=args.method,
+                                    flags=flags)
         for _ in range(3):
             p.execute(Ad, Bd, stream)
         a0 = torch.cuda.Event(enable_timing=True)

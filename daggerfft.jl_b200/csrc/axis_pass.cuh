@@ -260,15 +260,36 @@ template <typename V> struct StrideCol {
   __device__ __forceinline__ void st(int k, V v) const { p[k * s] = v; }
 };
 
+// Twiddle sources.  GlobalTw reads w_L^{jm*r*ts} from the L-entry table;
+// StageTw reads a stage-major table laid out [stage][jm][r-1] (entry
+// Ns - R_0 + jm*(R-1) + r-1 holds exp(-2 pi i jm r / (Ns R))), which the
+// persistent kernels keep in shared memory: lanes with consecutive jm read
+// consecutive (R-1)-strided entries, conflict-free.
+template <typename V> struct GlobalTw {
+  const V* p;
+  __device__ __forceinline__ V w(int off, int jm, int r, int R, int ts) const {
+    return ldg_c(p + jm * r * ts);
+  }
+};
+template <typename V> struct StageTw {
+  const V* p;
+  __device__ __forceinline__ V w(int off, int jm, int r, int R, int ts) const {
+    return p[off + jm * (R - 1) + r - 1];
+  }
+};
+
 // BMAX: upper bound on butterflies per thread; in the static kernels it is
 // exactly ceil((L/R)/P), in the dynamic kernel EMAX/R.
-// SMEM_IO: the first stage reads and the last stage writes the shared tile
-// (TMA kernels) instead of global memory.
-template <typename T, int R, int BMAX, bool FAST_IO, bool SMEM_IO, class COL>
-__device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int Ns, int ts,
-                                           bool first, bool last, int t, const COL& col,
-                                           const typename cvec<T>::type* tw,
-                                           long long ib, long long ob, bool cv) {
+// SMEM_IO: the first stage reads and the last stage writes shared memory
+// (pipelined kernels) instead of global memory.
+// CIN/COUT: the shared-memory views the stage reads and writes (they differ
+// when a stage moves a tile between a dense TMA buffer and a padded one).
+// toff: offset of this stage in a StageTw table (Ns - R_0).
+template <typename T, int R, int BMAX, bool FAST_IO, bool SMEM_IO, class CIN, class COUT, class TW>
+__device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int Ns, int ts, int toff,
+                                           bool first, bool last, int t, const CIN& cin,
+                                           const COUT& cout, const TW& tw, long long ib,
+                                           long long ob, bool cv) {
   typedef typename cvec<T>::type V;
   const int Lr = L / R;
   const bool to_global = !SMEM_IO && last && !d.epi;
@@ -289,7 +310,7 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
           if (d.inverse) x.y = -x.y;
           v[b][r] = x;
         } else {
-          V x = col.ld(k);
+          V x = cin.ld(k);
           if (SMEM_IO && first && d.inverse) x.y = -x.y;
           v[b][r] = x;
         }
@@ -304,7 +325,7 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
       const int jm = j % Ns;
       if (!first) {
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[b][r] = cmul(v[b][r], ldg_c(tw + jm * r * ts));
+        for (int r = 1; r < R; ++r) v[b][r] = cmul(v[b][r], tw.w(toff, jm, r, R, ts));
       }
       Dft<R>::run(v[b]);
       const int o0 = (j - jm) * R + jm;
@@ -321,9 +342,9 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
         } else if (SMEM_IO && last) {
           V y = v[b][r];
           if (d.inverse) y.y = -y.y;
-          col.st(k, cscale(y, (T)d.scale));
+          cout.st(k, cscale(y, (T)d.scale));
         } else {
-          col.st(k, v[b][r]);
+          cout.st(k, v[b][r]);
         }
       }
     }
@@ -374,18 +395,31 @@ __device__ __forceinline__ void r2c_epilogue(const PassDesc& d, int P, const Col
 // Static-plan kernel.
 // ---------------------------------------------------------------------------
 
-template <typename T, int L, int P, bool FAST_IO, bool SMEM_IO, int NS, int S, class COL, int R,
-          int... Rest>
-__device__ __forceinline__ void static_stages(const PassDesc& d, int t, const COL& col,
-                                              const typename cvec<T>::type* tw, long long ib,
-                                              long long ob, bool cv) {
+// Compile-time stage sequence.  The first stage reads CFIRST, the last
+// stage writes CLAST, every other access goes through CMID.
+template <typename T, int L, int P, bool FAST_IO, bool SMEM_IO, int NS, int R0, int S, class CFIRST,
+          class CMID, class CLAST, class TW, int R, int... Rest>
+__device__ __forceinline__ void static_stages(const PassDesc& d, int t, const CFIRST& cf,
+                                              const CMID& cm, const CLAST& cl, const TW& tw,
+                                              long long ib, long long ob, bool cv) {
   constexpr int Lr = L / R;
   constexpr int BM = (Lr + P - 1) / P;
   constexpr int TS = L / (NS * R);
-  stage_body<T, R, BM, FAST_IO, SMEM_IO>(d, L, P, NS, TS, S == 0, sizeof...(Rest) == 0, t, col, tw,
-                                         ib, ob, cv);
+  constexpr bool FIRST = (S == 0);
+  constexpr bool LAST = (sizeof...(Rest) == 0);
+  constexpr int R0_ = FIRST ? R : R0;
+  if constexpr (FIRST && LAST) {
+    stage_body<T, R, BM, FAST_IO, SMEM_IO>(d, L, P, NS, TS, NS - R0_, true, true, t, cf, cl, tw, ib, ob, cv);
+  } else if constexpr (FIRST) {
+    stage_body<T, R, BM, FAST_IO, SMEM_IO>(d, L, P, NS, TS, NS - R0_, true, false, t, cf, cm, tw, ib, ob, cv);
+  } else if constexpr (LAST) {
+    stage_body<T, R, BM, FAST_IO, SMEM_IO>(d, L, P, NS, TS, NS - R0_, false, true, t, cm, cl, tw, ib, ob, cv);
+  } else {
+    stage_body<T, R, BM, FAST_IO, SMEM_IO>(d, L, P, NS, TS, NS - R0_, false, false, t, cm, cm, tw, ib, ob, cv);
+  }
   if constexpr (sizeof...(Rest) > 0)
-    static_stages<T, L, P, FAST_IO, SMEM_IO, NS * R, S + 1, COL, Rest...>(d, t, col, tw, ib, ob, cv);
+    static_stages<T, L, P, FAST_IO, SMEM_IO, NS * R, R0_, S + 1, CFIRST, CMID, CLAST, TW, Rest...>(
+        d, t, cf, cm, cl, tw, ib, ob, cv);
 }
 
 template <typename T, bool FAST_IO, int LB, int L, int P, int... Rs>
@@ -395,8 +429,9 @@ __global__ void __launch_bounds__(LB) axis_pass_static(const PassDesc d) {
   V* sm = reinterpret_cast<V*>(smem_raw);
   const ColCtx x = col_ctx(d, P);
   const PadCol<V> col{sm + x.c * d.ld};
-  const V* tw = reinterpret_cast<const V*>(d.tw);
-  static_stages<T, L, P, FAST_IO, false, 1, 0, PadCol<V>, Rs...>(d, x.t, col, tw, x.ib, x.ob, x.cv);
+  const GlobalTw<V> tw{reinterpret_cast<const V*>(d.tw)};
+  static_stages<T, L, P, FAST_IO, false, 1, 1, 0, PadCol<V>, PadCol<V>, PadCol<V>, GlobalTw<V>, Rs...>(
+      d, x.t, col, col, col, tw, x.ib, x.ob, x.cv);
   if (!FAST_IO && d.epi) r2c_epilogue<T>(d, P, x, col.p);
 }
 
@@ -408,9 +443,11 @@ template <typename T, int R, int EMAX>
 __device__ __noinline__ void dyn_stage(const PassDesc& d, int s, int t, typename cvec<T>::type* col,
                                        const typename cvec<T>::type* tw, long long ib, long long ob,
                                        bool cv) {
-  const PadCol<typename cvec<T>::type> c{col};
-  stage_body<T, R, EMAX / R, false, false>(d, d.L, d.P, d.ns[s], d.tws[s], s == 0, s == d.nst - 1,
-                                           t, c, tw, ib, ob, cv);
+  typedef typename cvec<T>::type V;
+  const PadCol<V> c{col};
+  const GlobalTw<V> g{tw};
+  stage_body<T, R, EMAX / R, false, false>(d, d.L, d.P, d.ns[s], d.tws[s], 0, s == 0,
+                                           s == d.nst - 1, t, c, c, g, ib, ob, cv);
 }
 
 template <typename T, int EMAX>

@@ -93,6 +93,31 @@ int dfft_device_error(int* code) {
   });
 }
 
+int dfft_wisdom_export(const char* path) {
+  if (!path) { dfft::set_error("path is NULL"); return DFFT_ERROR_INVALID_VALUE; }
+  int st = dfft::wisdom_export(path);
+  if (st) dfft::set_error(std::string("cannot write wisdom file ") + path);
+  return st;
+}
+
+int dfft_wisdom_import(const char* path) {
+  if (!path) { dfft::set_error("path is NULL"); return DFFT_ERROR_INVALID_VALUE; }
+  int st = dfft::wisdom_import(path);
+  if (st) dfft::set_error(std::string("cannot read wisdom file ") + path);
+  return st;
+}
+
+int dfft_wisdom_forget(void) {
+  dfft::wisdom_forget();
+  return DFFT_SUCCESS;
+}
+
+int dfft_wisdom_size(int* n) {
+  if (!n) { dfft::set_error("n is NULL"); return DFFT_ERROR_INVALID_VALUE; }
+  *n = dfft::wisdom_size();
+  return DFFT_SUCCESS;
+}
+
 const char* dfft_last_error(void) { return dfft::last_error(); }
 
 const char* dfft_status_string(int status) {

@@ -44,7 +44,9 @@ struct Pass {
   size_t smem = 0;
   int src = BUF_IN, dst = BUF_OUT;
   bool is_static = false;
-  // TMA-pipelined strided pass: tensor {I*xscale, L, O} of 8-byte elements
+  // persistent pipelined pass (bulk copies); tma: strided, tensor
+  // {I*xscale, L, O} of 8-byte elements
+  bool pipe = false;
   bool tma = false;
   TmaGeom geom{};
   long long tI = 0, tL = 0, tO = 0;
@@ -53,6 +55,8 @@ struct Pass {
 
 // Device error word of the current device (bounded waits that expire set it).
 int* device_error_word();
+
+enum Variant : int { VARIANT_AUTO = 0, VARIANT_DIRECT = 1, VARIANT_PIPE = 2, VARIANT_DYNAMIC = 3 };
 
 // Pass construction.
 struct PassSpec {
@@ -64,10 +68,20 @@ struct PassSpec {
   IoAny in{}, out{};         // pointers filled at execute time
   bool epi = false;          // R2C half-length post-pass
   bool fast_io = false;      // plain complex in/out
+  int variant = VARIANT_AUTO;
+  int C = 0;                 // columns per CTA (0: heuristic)
 };
 
 // Builds a launchable pass; throws Error on unsupported sizes.
 Pass make_pass(const PassSpec& s);
+
+// Planner entry: wisdom lookup, tuning (DFFT_FLAG_TUNE) or heuristics.
+Pass plan_pass(const PassSpec& s, unsigned flags);
+Pass tune_pass(const PassSpec& s);
+int wisdom_export(const char* path);
+int wisdom_import(const char* path);
+void wisdom_forget();
+int wisdom_size();
 
 // Launches one pass on `stream` with the given buffers.
 cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream);

@@ -77,8 +77,8 @@ def launch_bound(dbl, E):
 
 
 def has_tma(dt, n):
-    """Strided C2C lengths that get a TMA-pipelined kernel (three tile
-    buffers of at least 4 columns must fit in shared memory)."""
+    """C2C lengths that get the TMA-pipelined kernels (three tile buffers of
+    at least 4 columns must fit in shared memory)."""
     esz = 8 if dt == "float" else 16
     return 8 <= n and 3 * 4 * n * esz + 128 <= 227 * 1024 and n <= (1024 if dt == "float" else 512)
 
@@ -115,9 +115,10 @@ def main():
                 lines.append(f"template __global__ void axis_pass_static<{dt},false,{lb},{n},{P},{rs}>(const PassDesc);")
                 if has_tma(dt, n):
                     tlb = tma_bound(dt, lb)
-                    lines.append(f"template __global__ void axis_pass_tma<{dt},{tlb},{n},{P},{rs}>("
-                                 "const PassDesc, const __grid_constant__ CUtensorMap, "
-                                 "const __grid_constant__ CUtensorMap, const TmaGeom);")
+                    for cg in ("false", "true"):
+                        lines.append(f"template __global__ void axis_pass_pipe<{dt},{tlb},{cg},{n},{P},{rs}>("
+                                     "const PassDesc, const __grid_constant__ CUtensorMap, "
+                                     "const __grid_constant__ CUtensorMap, const TmaGeom);")
             lines.append(f"extern const StaticPlan kPlans_{tag}_{fi}[];")
             lines.append(f"extern const int kPlansCount_{tag}_{fi};")
             lines.append(f"const StaticPlan kPlans_{tag}_{fi}[] = {{")
@@ -125,12 +126,14 @@ def main():
                 rs = ",".join(str(r) for r in rad)
                 radarr = "{" + ",".join(str(r) for r in rad) + "}"
                 tlb = tma_bound(dt, lb)
-                tma = (f"(const void*)&axis_pass_tma<{dt},{tlb},{n},{P},{rs}>" if has_tma(dt, n)
-                       else "nullptr")
+                ps = (f"(const void*)&axis_pass_pipe<{dt},{tlb},false,{n},{P},{rs}>" if has_tma(dt, n)
+                      else "nullptr")
+                pc = (f"(const void*)&axis_pass_pipe<{dt},{tlb},true,{n},{P},{rs}>" if has_tma(dt, n)
+                      else "nullptr")
                 lines.append(
                     f"  {{{n}, {P}, {len(rad)}, {radarr}, {lb}, "
                     f"(const void*)&axis_pass_static<{dt},true,{lb},{n},{P},{rs}>, "
-                    f"(const void*)&axis_pass_static<{dt},false,{lb},{n},{P},{rs}>, {tma}, {tlb}}},")
+                    f"(const void*)&axis_pass_static<{dt},false,{lb},{n},{P},{rs}>, {ps}, {pc}, {tlb}}},")
             lines.append("};")
             lines.append(f"const int kPlansCount_{tag}_{fi} = {len(ch)};")
             lines.append("}  // namespace dfft")

@@ -229,21 +229,85 @@ static size_t max_smem_per_block() {
   return v;
 }
 
+// Stage-major twiddle table for a radix sequence (StageTw layout): entry
+// Ns - R_0 + jm*(R-1) + r-1 of stage s >= 1 is exp(-2 pi i jm r / (Ns R)).
+static std::shared_ptr<DevTable> stage_twiddles(int dbl, int L, const std::vector<int>& rad) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, std::vector<int>>, std::weak_ptr<DevTable>> cache;
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  auto key = std::make_tuple(dev * 2 + dbl, L, rad);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(key);
+  if (it != cache.end())
+    if (auto sp = it->second.lock()) return sp;
+  const int R0 = rad.empty() ? 1 : rad[0];
+  const int n = L - R0 > 0 ? L - R0 : 1;
+  const size_t esz = dbl ? 16 : 8;
+  std::vector<unsigned char> host(esz * (size_t)n, 0);
+  const long double two_pi = 2.0L * acosl(-1.0L);
+  int Ns = R0;
+  for (size_t st = 1; st < rad.size(); ++st) {
+    const int R = rad[st];
+    for (int jm = 0; jm < Ns; ++jm)
+      for (int r = 1; r < R; ++r) {
+        const long long D = (long long)Ns * R;
+        const long long m = ((long long)jm * r) % D;
+        const long double ang = two_pi * (long double)m / (long double)D;
+        const long double c = cosl(ang), sn = -sinl(ang);
+        const size_t e = (size_t)(Ns - R0 + jm * (R - 1) + r - 1);
+        if (dbl) { double v[2] = {(double)c, (double)sn}; std::memcpy(&host[esz * e], v, esz); }
+        else { float v[2] = {(float)c, (float)sn}; std::memcpy(&host[esz * e], v, esz); }
+      }
+    Ns *= R;
+  }
+  auto t = std::make_shared<DevTable>();
+  t->device = dev;
+  t->bytes = host.size();
+  cuda_check(cudaMalloc(&t->p, t->bytes), "cudaMalloc(stage twiddles)");
+  cuda_check(cudaMemcpy(t->p, host.data(), t->bytes, cudaMemcpyHostToDevice), "cudaMemcpy(stage twiddles)");
+  cache[key] = t;
+  return t;
+}
+
+// Which kernel a pass may use.
+static bool pipe_strided_ok(const PassSpec& s, const StaticPlan* sp, size_t esz) {
+  return sp && sp->pipe_s && s.fast_io && !s.epi && s.I > 1 && (s.I * (long long)esz) % 16 == 0 &&
+         s.I < (1LL << 31) && s.O < (1LL << 31);
+}
+static bool pipe_contig_ok(const PassSpec& s, const StaticPlan* sp, size_t esz) {
+  return sp && sp->pipe_c && s.fast_io && !s.epi && s.I == 1 && ((long long)s.L * (long long)esz) % 16 == 0;
+}
+
 Pass make_pass(const PassSpec& s) {
   Pass p;
   PassDesc& d = p.d;
   const int L = s.L;
   if (L < 1) throw Error{DFFT_ERROR_INVALID_VALUE, "transform length must be >= 1"};
+  const int esz = s.dbl ? 16 : 8;
+  const size_t smax = max_smem_per_block();
   const StaticPlan* sp = find_static(s.dbl, L);
+  if (sp && sp->P > sp->lb) sp = nullptr;
+  int variant = s.variant;
+  if (variant == VARIANT_AUTO) {
+    if (pipe_strided_ok(s, sp, esz) || pipe_contig_ok(s, sp, esz)) {
+      PassSpec t = s;
+      t.variant = VARIANT_PIPE;
+      try {
+        return make_pass(t);
+      } catch (const Error&) {
+      }
+    }
+    variant = sp ? VARIANT_DIRECT : VARIANT_DYNAMIC;
+  }
+  if (variant == VARIANT_PIPE && !(pipe_strided_ok(s, sp, esz) || pipe_contig_ok(s, sp, esz)))
+    throw Error{DFFT_ERROR_INVALID_VALUE, "pipelined variant not available for this pass"};
+  if (variant == VARIANT_DIRECT && !sp)
+    throw Error{DFFT_ERROR_INVALID_VALUE, "no static plan for this length"};
+
   std::vector<int> rad;
   int P = 0, lb = 1024;
-  if (sp && sp->P <= sp->lb) {
-    rad.assign(sp->radix, sp->radix + sp->nst);
-    P = sp->P;
-    lb = sp->lb;
-    p.fn = s.fast_io ? sp->fast : sp->any;
-    p.is_static = true;
-  } else {
+  if (variant == VARIANT_DYNAMIC) {
     rad = dynamic_radices(L);
     if (rad.empty())
       throw Error{DFFT_ERROR_UNSUPPORTED_SIZE,
@@ -257,9 +321,17 @@ Pass make_pass(const PassSpec& s) {
     }
     lb = 1024;
     p.fn = dynamic_kernel(s.dbl);
+  } else {
+    rad.assign(sp->radix, sp->radix + sp->nst);
+    P = sp->P;
+    lb = variant == VARIANT_PIPE ? sp->pipe_lb : sp->lb;
+    p.is_static = true;
+    if (variant == VARIANT_DIRECT) p.fn = s.fast_io ? sp->fast : sp->any;
   }
   if ((int)rad.size() > kMaxStages)
     throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "too many stages for length " + std::to_string(L)};
+  if (P > lb)
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "length " + std::to_string(L) + " exceeds one CTA"};
   d.L = L;
   d.nst = (int)rad.size();
   int ns = 1;
@@ -270,69 +342,114 @@ Pass make_pass(const PassSpec& s) {
     ns *= rad[i];
   }
   d.P = P;
-  if (P > lb)
-    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "length " + std::to_string(L) + " exceeds one CTA"};
-  const int esz = s.dbl ? 16 : 8;
   int ld = swz_host(L - 1, esz) + 1;
   if ((ld & 1) == 0) ld += 1;
   d.ld = ld;
   d.cfast = s.I > 1 ? 1 : 0;
-  const size_t smax = max_smem_per_block();
+  d.inverse = s.inverse;
+  d.epi = s.epi ? 1 : 0;
+  const long long Q = s.I * s.O;
+  d.Q = Q;
+  d.I = s.I;
+  d.scale = s.scale;
+  d.in = s.in;
+  d.out = s.out;
   const size_t col_bytes = (size_t)ld * esz;
+
+  if (variant == VARIANT_PIPE) {
+    const bool contig = s.I == 1;
+    p.fn = contig ? sp->pipe_c : sp->pipe_s;
+    p.tma = !contig;
+    p.pipe = true;
+    auto stw = stage_twiddles(s.dbl, L, rad);
+    p.tables.push_back(stw);
+    d.tw = stw->p;
+    TmaGeom& g = p.geom;
+    g.ntw = d.nst > 1 ? L - rad[0] : 0;
+    const size_t tw_bytes = ((size_t)g.ntw * esz + 127) & ~(size_t)127;
+    auto bstride_bytes = [&](int C) { return ((size_t)C * L * esz + 127) & ~(size_t)127; };
+    auto smem_for = [&](int C) {
+      return 128 + tw_bytes + (size_t)kTmaBufs * bstride_bytes(C) + (contig ? (size_t)C * ld * esz : 0);
+    };
+    int C = s.C;
+    if (C <= 0) {
+      if (contig) {
+        C = 1;
+        while (C * 2 * P <= 256 && smem_for(C * 2) <= smax) C *= 2;
+      } else {
+        C = s.dbl ? 8 : 16;
+        while (C * P < 256 && C < 64 && smem_for(C * 2) <= smax) C *= 2;
+      }
+    }
+    while (C > 1 && (C * P > lb || smem_for(C) > smax)) C /= 2;
+    if (!contig && C % 2) C = 2;  // 16-byte TMA rows for complex float
+    if (C * P > lb || smem_for(C) > smax)
+      throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "pipelined tile does not fit"};
+    if (!contig) {
+      // every TMA box must start 128 bytes apart inside the tile buffer
+      const int lbr = box_rows(L);
+      if (L / lbr > 1 && ((size_t)lbr * C * esz) % 128 != 0)
+        throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "TMA box offsets would not be 128-byte aligned"};
+    }
+    d.C = C;
+    g.C = C;
+    g.xscale = s.dbl ? 2 : 1;
+    g.ld = ld;
+    g.bstride = (int)(bstride_bytes(C) / esz);
+    g.err = device_error_word();
+    if (contig) {
+      g.ncols = Q;
+      g.ntiles = (Q + C - 1) / C;
+      g.tiles_i = 1;
+      g.lb = L;
+      g.nlb = 1;
+      g.tile_bytes = (unsigned)((size_t)C * L * esz);
+    } else {
+      p.tI = s.I;
+      p.tL = L;
+      p.tO = s.O;
+      g.tiles_i = (int)((s.I + C - 1) / C);
+      g.ntiles = (long long)g.tiles_i * s.O;
+      g.ncols = Q;
+      g.lb = box_rows(L);
+      g.nlb = L / g.lb;
+      g.tile_bytes = (unsigned)((size_t)C * L * esz);
+    }
+    p.block = dim3((unsigned)(C * P));
+    p.smem = smem_for(C);
+    cuda_check(ensure_smem_attr(p.fn, p.smem), "cudaFuncSetAttribute(pipe)");
+    int occ = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p.fn, (int)p.block.x, p.smem),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (occ < 1) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "pipelined kernel cannot be resident"};
+    long long nb = (long long)sm_count() * occ;
+    if (nb > g.ntiles) nb = g.ntiles;
+    p.grid = dim3((unsigned)(nb > 0 ? nb : 1));
+    return p;
+  }
+
   if (col_bytes > smax)
     throw Error{DFFT_ERROR_UNSUPPORTED_SIZE,
                 "length " + std::to_string(L) + " does not fit one CTA's shared memory"};
-  int C;
-  if (d.cfast) {
-    // rows of at least 128 bytes for coalesced strided loads, ~256 threads
-    C = s.dbl ? 8 : 16;
-    while (C * P < 256 && C < 64) C *= 2;
-  } else {
-    C = 1;
-    while (C * 2 * P <= 256) C *= 2;
+  int C = s.C;
+  if (C <= 0) {
+    if (d.cfast) {
+      // rows of at least 128 bytes for coalesced strided loads, ~256 threads
+      C = s.dbl ? 8 : 16;
+      while (C * P < 256 && C < 64) C *= 2;
+    } else {
+      C = 1;
+      while (C * 2 * P <= 256) C *= 2;
+    }
   }
   while (C > 1 && (C * P > lb || (size_t)C * col_bytes > smax)) C /= 2;
-  const long long Q = s.I * s.O;
   if (Q > 0 && C > Q) {
     // do not launch threads for columns that do not exist
     int c2 = 1;
     while (c2 * 2 <= Q) c2 *= 2;
     if (c2 < C) C = c2;
   }
-  // TMA-pipelined variant for strided C2C passes (8-byte TMA elements need
-  // 16-byte row strides; three tile buffers must fit in shared memory)
-  if (p.is_static && sp->tma && s.fast_io && s.I > 1 && (s.I * esz) % 16 == 0 && s.I < (1LL << 31) &&
-      s.O < (1LL << 31) && (s.I + C - 1) / C < (1LL << 31)) {
-    int Ct = s.dbl ? 8 : 16;
-    while (Ct * P < 256 && Ct < 64 && (size_t)kTmaBufs * 2 * Ct * L * esz + 128 <= smax) Ct *= 2;
-    const int tlb = sp->tma_lb;
-    while (Ct > 4 && (Ct * P > tlb || (size_t)kTmaBufs * Ct * L * esz + 128 > smax)) Ct /= 2;
-    if (Ct * P <= tlb && (size_t)kTmaBufs * Ct * L * esz + 128 <= smax) {
-      p.tma = true;
-      p.fn = sp->tma;
-      p.tI = s.I;
-      p.tL = L;
-      p.tO = s.O;
-      TmaGeom& g = p.geom;
-      g.C = Ct;
-      g.tiles_i = (int)((s.I + Ct - 1) / Ct);
-      g.ntiles = (long long)g.tiles_i * s.O;
-      g.lb = box_rows(L);
-      g.nlb = L / g.lb;
-      g.xscale = s.dbl ? 2 : 1;
-      g.tile_bytes = (unsigned)((size_t)Ct * L * esz);
-      g.err = device_error_word();
-      C = Ct;
-    }
-  }
   d.C = C;
-  d.inverse = s.inverse;
-  d.epi = s.epi ? 1 : 0;
-  d.Q = Q;
-  d.I = s.I;
-  d.scale = s.scale;
-  d.in = s.in;
-  d.out = s.out;
   auto tw = twiddle_table(s.dbl, L, 1, 0, L, false);
   p.tables.push_back(tw);
   d.tw = tw->p;
@@ -340,19 +457,6 @@ Pass make_pass(const PassSpec& s) {
     auto tw2 = twiddle_table(s.dbl, 2LL * L, 1, 0, L + 1, false);
     p.tables.push_back(tw2);
     d.tw2 = tw2->p;
-  }
-  if (p.tma) {
-    p.block = dim3((unsigned)(C * P));
-    p.smem = 128 + (size_t)kTmaBufs * C * L * esz;
-    cuda_check(ensure_smem_attr(p.fn, p.smem), "cudaFuncSetAttribute(tma)");
-    int occ = 0;
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p.fn, (int)p.block.x, p.smem),
-               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (occ < 1) occ = 1;
-    long long nb = (long long)sm_count() * occ;
-    if (nb > p.geom.ntiles) nb = p.geom.ntiles;
-    p.grid = dim3((unsigned)(nb > 0 ? nb : 1));
-    return p;
   }
   const long long nblk = (Q + C - 1) / C;
   if (nblk > 0x7fffffffLL) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "too many columns for one launch"};
@@ -369,14 +473,18 @@ cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream)
   PassDesc d = p.d;
   d.in.p = in;
   d.out.p = out;
-  if (p.tma) {
+  if (p.pipe) {
     if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
       return cudaErrorMisalignedAddress;
     CUtensorMap tin, tout;
-    e = encode_map(&tin, in, p);
-    if (e != cudaSuccess) return e;
-    e = encode_map(&tout, out, p);
-    if (e != cudaSuccess) return e;
+    std::memset(&tin, 0, sizeof(tin));
+    std::memset(&tout, 0, sizeof(tout));
+    if (p.tma) {
+      e = encode_map(&tin, in, p);
+      if (e != cudaSuccess) return e;
+      e = encode_map(&tout, out, p);
+      if (e != cudaSuccess) return e;
+    }
     TmaGeom g = p.geom;
     void* args[] = {&d, &tin, &tout, &g};
     return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);

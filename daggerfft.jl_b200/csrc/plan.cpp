@@ -98,7 +98,7 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
       s.in = io(IO_CPLX, s.I, S[a]);
       s.out = io(IO_CPLX, s.I, S[a]);
       s.fast_io = true;
-      Pass p = make_pass(s);
+      Pass p = plan_pass(s, flags);
       p.src = src;
       p.dst = BUF_OUT;
       src = BUF_OUT;
@@ -127,7 +127,7 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
       s.out = io(IO_TRUNC, s.I, H[a0]);
       s.out.n = (int)(n / 2);
     }
-    Pass p0 = make_pass(s);
+    Pass p0 = plan_pass(s, flags);
     p0.src = BUF_IN;
     p0.dst = BUF_OUT;
     P->passes.push_back(std::move(p0));
@@ -140,7 +140,7 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
       c.in = io(IO_CPLX, c.I, H[a]);
       c.out = io(IO_CPLX, c.I, H[a]);
       c.fast_io = true;
-      Pass p = make_pass(c);
+      Pass p = plan_pass(c, flags);
       p.src = BUF_OUT;
       p.dst = BUF_OUT;
       P->passes.push_back(std::move(p));
@@ -172,7 +172,7 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
       c.in = io(IO_CPLX, c.I, S[a]);
       c.out = io(IO_CPLX, c.I, S[a]);
       c.fast_io = true;
-      Pass p = make_pass(c);
+      Pass p = plan_pass(c, flags);
       p.src = src;
       p.dst = work;
       src = work;
@@ -197,7 +197,7 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
       s.in.n = (int)d;
       s.out = io(IO_REAL, s.I, d);
     }
-    Pass p = make_pass(s);
+    Pass p = plan_pass(s, flags);
     if (d % 2 == 0) {
       auto w = twiddle_table(dbl, d, 1, 0, (int)(d / 2) + 1, false);
       p.tables.push_back(w);
@@ -253,7 +253,7 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
         default:
           throw Error{DFFT_ERROR_UNKNOWN_TRANSFORM, "Unknown transform type"};
       }
-      Pass p = make_pass(s);
+      Pass p = plan_pass(s, flags);
       if (win) { p.tables.push_back(win); p.d.in.w = win->p; }
       if (wout) { p.tables.push_back(wout); p.d.out.w = wout->p; }
       p.src = src;

@@ -12,8 +12,9 @@ struct StaticPlan {
   int lb;             // __launch_bounds__ of the kernels (max threads per CTA)
   const void* fast;   // axis_pass_static<T, true, ...>: complex in, complex out
   const void* any;    // axis_pass_static<T, false, ...>: any IoKind, R2C post-pass
-  const void* tma;    // axis_pass_tma<T, ...>: strided C2C, TMA-pipelined (or null)
-  int tma_lb;         // __launch_bounds__ of the TMA kernel
+  const void* pipe_s; // axis_pass_pipe<T, LB, false, ...>: strided C2C, TMA-pipelined (or null)
+  const void* pipe_c; // axis_pass_pipe<T, LB, true, ...>: contiguous C2C, bulk-copy pipelined
+  int pipe_lb;        // __launch_bounds__ of the pipelined kernels
 };
 
 struct StaticPlanTable {

@@ -1,22 +1,32 @@
-// Persistent, TMA-pipelined pass for the strided axes of a C2C transform.
+// Persistent, TMA-pipelined passes.
 //
-// A tile is C adjacent columns x L rows (row k of the tile is C contiguous
-// complex elements at i0 + k*I + o*I*L).  It is moved by the Tensor Memory
-// Accelerator as a 3-D box {C, Lb, 1} of the tensor {I, L, O}: the box lands
-// in shared memory as [k][c] (c fastest), which the cfast thread mapping
-// reads and writes without bank conflicts in every Stockham stage, and the
-// finished tile leaves the same buffer through a bulk-tensor store.
+// Strided axes (CONTIG = false).  A tile is C adjacent columns x L rows (row
+// k of the tile is C contiguous complex elements at i0 + k*I + o*I*L).  The
+// Tensor Memory Accelerator moves it as 3-D boxes {C, Lb, 1} of the tensor
+// {I, L, O}: the boxes land in shared memory as [k][c] (c fastest), which the
+// cfast thread mapping reads and writes without bank conflicts in every
+// Stockham stage, and the finished tile leaves the same buffer through a
+// bulk-tensor store.
 //
-// Each CTA owns NBUF tile buffers and walks tiles blockIdx.x, +gridDim.x, ...
-// While it computes tile i, the loads of tiles i+1 .. i+NBUF-1 are in flight
-// and the store of tile i-1 drains, so HBM traffic overlaps the shared-memory
-// FFT.  Ordering: threads write the tile, fence.proxy.async, barrier, then one
-// thread issues the store; a buffer is reloaded only after
+// Contiguous axis (CONTIG = true).  A tile is C whole pencils, one contiguous
+// run of C*L elements moved by a 1-D bulk copy.  It lands dense ([c][k]);
+// the first stage reads it there and writes a padded work buffer (the
+// stride-R writes of the early stages would conflict in the dense layout),
+// the middle stages stay in the work buffer, and the last stage (whose writes
+// are unit-stride) puts the result back into the dense buffer for the bulk
+// store.
+//
+// Each CTA owns kTmaBufs tile buffers and walks tiles blockIdx.x, +gridDim.x,
+// ...  While it computes tile i, the loads of tiles i+1 .. i+kTmaBufs-1 are in
+// flight and the store of tile i-1 drains, so HBM traffic overlaps the
+// shared-memory FFT.  Ordering: threads write the tile, fence.proxy.async,
+// barrier, then one thread issues the store; a buffer is reloaded only after
 // cp.async.bulk.wait_group.read confirms its previous store has read it.
+// Stage twiddles are copied once per CTA into shared memory (StageTw layout).
 //
-// Every mbarrier wait is bounded; on expiry the kernel records
-// DFFT_DEVERR_TMA_TIMEOUT in the device error word, drains its own copies
-// (bounded) and returns.
+// Every mbarrier wait is bounded (~2 s); on expiry the kernel records
+// DFFT_DEVERR_TMA_TIMEOUT in the device error word, waits (bounded) for the
+// copies it issued and returns.
 #pragma once
 #include <cuda.h>
 #include "axis_pass.cuh"
@@ -24,17 +34,21 @@
 namespace dfft {
 
 constexpr int kTmaBufs = 3;
-constexpr unsigned kWaitLimit = 1u << 26;   // try_wait rounds before giving up
+constexpr unsigned kWaitLimit = 1u << 26;    // try_wait rounds before giving up
 constexpr uint64_t kWaitNs = 2000000000ull;  // and at most ~2 s of wall time
-enum : int { DFFT_DEVERR_TMA_TIMEOUT = 1 };
+enum : int { DFFT_DEVERR_TMA_TIMEOUT = 1, DFFT_DEVERR_TMA_ALIGN = 2 };
 
 struct TmaGeom {
-  int C;              // columns per tile
-  int tiles_i;        // tiles along the inner extent I
-  long long ntiles;   // tiles_i * O
-  int lb;             // rows per TMA box (<= 256)
-  int nlb;            // boxes per tile (L / lb)
+  int C;              // columns (strided) or pencils (contiguous) per tile
+  int tiles_i;        // strided: tiles along the inner extent I
+  long long ntiles;   // number of tiles
+  long long ncols;    // contiguous: number of pencils
+  int lb;             // strided: rows per TMA box (<= 256)
+  int nlb;            // strided: boxes per tile (L / lb)
   int xscale;         // TMA x units per column: 1 (complex float), 2 (complex double)
+  int ld;             // contiguous: padded work-buffer elements per pencil
+  int ntw;            // stage-twiddle entries to stage in shared memory
+  int bstride;        // elements between tile buffers (a multiple of 128 bytes)
   unsigned tile_bytes;
   int* err;           // device error word
 };
@@ -91,6 +105,18 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void*
                ::"l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
                : "memory");
 }
+__device__ __forceinline__ void bulk_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void bulk_store_1d(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+               "r"(smem_u32(src)), "r"(bytes)
+               : "memory");
+}
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read_all() {
   asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
@@ -100,55 +126,93 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-template <typename V>
-__device__ __forceinline__ void tma_issue_tile_load(const CUtensorMap* map, V* buf, uint64_t* bar,
-                                                    const TmaGeom& g, long long tile, int C) {
-  const int ti = (int)(tile % g.tiles_i);
-  const int o = (int)(tile / g.tiles_i);
-  mbar_expect_tx(bar, g.tile_bytes);
-  for (int b = 0; b < g.nlb; ++b)
-    tma_load_3d(buf + (size_t)b * g.lb * C, map, bar, ti * C * g.xscale, b * g.lb, o);
+template <typename V, bool CONTIG, int L>
+__device__ __forceinline__ void pipe_issue_load(const PassDesc& d, const CUtensorMap* map, V* buf,
+                                                uint64_t* bar, const TmaGeom& g, long long tile) {
+  if (CONTIG) {
+    const long long q0 = tile * g.C;
+    const long long nv = (g.ncols - q0) < g.C ? (g.ncols - q0) : g.C;
+    const uint32_t bytes = (uint32_t)(nv * L * (long long)sizeof(V));
+    mbar_expect_tx(bar, bytes);
+    bulk_load_1d(buf, reinterpret_cast<const V*>(d.in.p) + q0 * L, bytes, bar);
+  } else {
+    const int ti = (int)(tile % g.tiles_i);
+    const int o = (int)(tile / g.tiles_i);
+    mbar_expect_tx(bar, g.tile_bytes);
+    for (int b = 0; b < g.nlb; ++b)
+      tma_load_3d(buf + (size_t)b * g.lb * g.C, map, bar, ti * g.C * g.xscale, b * g.lb, o);
+  }
 }
 
-template <typename V>
-__device__ __forceinline__ void tma_issue_tile_store(const CUtensorMap* map, const V* buf,
-                                                     const TmaGeom& g, long long tile, int C) {
-  const int ti = (int)(tile % g.tiles_i);
-  const int o = (int)(tile / g.tiles_i);
-  for (int b = 0; b < g.nlb; ++b)
-    tma_store_3d(map, buf + (size_t)b * g.lb * C, ti * C * g.xscale, b * g.lb, o);
+template <typename V, bool CONTIG, int L>
+__device__ __forceinline__ void pipe_issue_store(const PassDesc& d, const CUtensorMap* map,
+                                                 const V* buf, const TmaGeom& g, long long tile) {
+  if (CONTIG) {
+    const long long q0 = tile * g.C;
+    const long long nv = (g.ncols - q0) < g.C ? (g.ncols - q0) : g.C;
+    bulk_store_1d(reinterpret_cast<V*>(d.out.p) + q0 * L, buf, (uint32_t)(nv * L * (long long)sizeof(V)));
+  } else {
+    const int ti = (int)(tile % g.tiles_i);
+    const int o = (int)(tile / g.tiles_i);
+    for (int b = 0; b < g.nlb; ++b)
+      tma_store_3d(map, buf + (size_t)b * g.lb * g.C, ti * g.C * g.xscale, b * g.lb, o);
+  }
 }
 
-template <typename T, int LB, int L, int P, int... Rs>
-__global__ void __launch_bounds__(LB) axis_pass_tma(const PassDesc d,
-                                                    const __grid_constant__ CUtensorMap tin,
-                                                    const __grid_constant__ CUtensorMap tout,
-                                                    const TmaGeom g) {
+// Shared-memory layout of the pipelined kernels (bytes):
+//   [0, 128)                  kTmaBufs mbarriers; abort flag at byte 64
+//   [128, 128 + tw)           stage twiddles (ntw entries, padded to 128 bytes)
+//   then kTmaBufs tile buffers of C*L elements, bstride apart
+//   then (CONTIG) one padded work buffer of C*ld elements
+// Bulk-tensor copies need 128-byte aligned shared addresses: the twiddle
+// region, the buffer stride and (host-checked) every box offset inside a
+// buffer are multiples of 128 bytes; the kernel re-checks and reports
+// DFFT_DEVERR_TMA_ALIGN instead of issuing a misaligned copy.
+template <typename T, int LB, bool CONTIG, int L, int P, int... Rs>
+__global__ void __launch_bounds__(LB) axis_pass_pipe(const PassDesc d,
+                                                     const __grid_constant__ CUtensorMap tin,
+                                                     const __grid_constant__ CUtensorMap tout,
+                                                     const TmaGeom g) {
   typedef typename cvec<T>::type V;
-  extern __shared__ __align__(128) unsigned char smem_tma[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_tma);
-  __shared__ int s_abort;
-  V* bufs = reinterpret_cast<V*>(smem_tma + 128);
-  const int C = g.C;
-  const size_t buf_elems = (size_t)C * L;
+  extern __shared__ __align__(128) unsigned char smem_pipe[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_pipe);
+  int& s_abort = *reinterpret_cast<int*>(smem_pipe + 64);  // inside the barrier block
+  V* stw = reinterpret_cast<V*>(smem_pipe + 128);
+  const size_t tw_bytes = ((size_t)g.ntw * sizeof(V) + 127) & ~(size_t)127;
+  V* bufs = reinterpret_cast<V*>(smem_pipe + 128 + tw_bytes);
+  const size_t buf_elems = (size_t)g.bstride;
+  V* work = bufs + kTmaBufs * buf_elems;
   const int tid = threadIdx.x;
-  const int c = tid % C;
-  const int t = tid / C;
-  const V* tw = reinterpret_cast<const V*>(d.tw);
+  int c, t;
+  if (CONTIG) { t = tid % P; c = tid / P; }
+  else { c = tid % g.C; t = tid / g.C; }
   if (tid == 0) {
     for (int b = 0; b < kTmaBufs; ++b) mbar_init(&bars[b], 1);
     mbar_fence_init();
     s_abort = 0;
+    const uint32_t a0 = smem_u32(bufs);
+    const uint32_t bs = (uint32_t)(buf_elems * sizeof(V));
+    const uint32_t box = CONTIG ? 0u : (uint32_t)((size_t)g.lb * g.C * sizeof(V));
+    const uint32_t need = CONTIG ? 15u : 127u;
+    if ((a0 & need) || (bs & need) || (g.nlb > 1 && (box & 127u))) {
+      atomicExch(g.err, DFFT_DEVERR_TMA_ALIGN);
+      s_abort = 1;
+    }
   }
+  const V* gtw = reinterpret_cast<const V*>(d.tw);
+  for (int i = tid; i < g.ntw; i += blockDim.x) stw[i] = gtw[i];
   __syncthreads();
+  if (s_abort) return;  // misaligned layout: nothing was issued
+  const int C = g.C;
+  const StageTw<V> tw{stw};
   const long long first = blockIdx.x;
   const long long step = gridDim.x;
-  int issued[kTmaBufs] = {0, 0, 0};   // loads issued per buffer (thread 0)
+  int issued[kTmaBufs] = {0, 0, 0};  // loads issued per buffer (thread 0)
   if (tid == 0) {
     for (int b = 0; b < kTmaBufs - 1; ++b) {
       const long long tile = first + b * step;
       if (tile < g.ntiles) {
-        tma_issue_tile_load(&tin, bufs + b * buf_elems, &bars[b], g, tile, C);
+        pipe_issue_load<V, CONTIG, L>(d, &tin, bufs + b * buf_elems, &bars[b], g, tile);
         ++issued[b];
       }
     }
@@ -161,8 +225,16 @@ __global__ void __launch_bounds__(LB) axis_pass_tma(const PassDesc d,
     __syncthreads();
     if (s_abort) break;
     V* sb = bufs + buf * buf_elems;
-    const StrideCol<V> col{sb + c, C};
-    static_stages<T, L, P, true, true, 1, 0, StrideCol<V>, Rs...>(d, t, col, tw, 0, 0, true);
+    if (CONTIG) {
+      const StrideCol<V> dense{sb + (size_t)c * L, 1};
+      const PadCol<V> pad{work + (size_t)c * g.ld};
+      static_stages<T, L, P, true, true, 1, 1, 0, StrideCol<V>, PadCol<V>, StrideCol<V>, StageTw<V>,
+                    Rs...>(d, t, dense, pad, dense, tw, 0, 0, true);
+    } else {
+      const StrideCol<V> col{sb + c, C};
+      static_stages<T, L, P, true, true, 1, 1, 0, StrideCol<V>, StrideCol<V>, StrideCol<V>,
+                    StageTw<V>, Rs...>(d, t, col, col, col, tw, 0, 0, true);
+    }
     fence_proxy_async_smem();
     __syncthreads();
     if (tid == 0) {
@@ -171,10 +243,10 @@ __global__ void __launch_bounds__(LB) axis_pass_tma(const PassDesc d,
       const long long next = tile + (long long)(kTmaBufs - 1) * step;
       if (next < g.ntiles) {
         const int nb = (it + kTmaBufs - 1) % kTmaBufs;
-        tma_issue_tile_load(&tin, bufs + nb * buf_elems, &bars[nb], g, next, C);
+        pipe_issue_load<V, CONTIG, L>(d, &tin, bufs + nb * buf_elems, &bars[nb], g, next);
         ++issued[nb];
       }
-      tma_issue_tile_store(&tout, sb, g, tile, C);
+      pipe_issue_store<V, CONTIG, L>(d, &tout, sb, g, tile);
       bulk_commit();
     }
   }
@@ -182,9 +254,8 @@ __global__ void __launch_bounds__(LB) axis_pass_tma(const PassDesc d,
     bulk_wait_all();
     if (s_abort) {
       atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
-      // loads still in flight land in this CTA's shared memory: wait for
-      // the last load issued into each buffer (bounded) before the CTA
-      // releases it
+      // loads still in flight land in this CTA's shared memory: wait for the
+      // last load issued into each buffer (bounded) before the CTA exits
       for (int b = 0; b < kTmaBufs; ++b)
         if (issued[b] > 0) mbar_wait_bounded(&bars[b], (uint32_t)((issued[b] - 1) & 1));
     }

@@ -82,6 +82,13 @@ def lib():
     L.dfft_plan_destroy.restype = c_int
     L.dfft_device_error.argtypes = [ctypes.POINTER(c_int)]
     L.dfft_device_error.restype = c_int
+    for nm in ("dfft_wisdom_export", "dfft_wisdom_import"):
+        getattr(L, nm).argtypes = [c_char_p]
+        getattr(L, nm).restype = c_int
+    L.dfft_wisdom_forget.argtypes = []
+    L.dfft_wisdom_forget.restype = c_int
+    L.dfft_wisdom_size.argtypes = [ctypes.POINTER(c_int)]
+    L.dfft_wisdom_size.restype = c_int
     L.dfft_last_error.argtypes = []
     L.dfft_last_error.restype = c_char_p
     L.dfft_status_string.argtypes = [c_int]
@@ -116,4 +123,24 @@ def device_error():
     """Reads and clears the device error word (0 = no kernel gave up a wait)."""
     v = ctypes.c_int()
     check(lib().dfft_device_error(ctypes.byref(v)))
+    return v.value
+
+
+def wisdom_export(path):
+    """Writes the tuning cache (FFTW-wisdom analogue) to ``path``."""
+    check(lib().dfft_wisdom_export(str(path).encode()))
+
+
+def wisdom_import(path):
+    """Merges a tuning cache written by ``wisdom_export``."""
+    check(lib().dfft_wisdom_import(str(path).encode()))
+
+
+def wisdom_forget():
+    check(lib().dfft_wisdom_forget())
+
+
+def wisdom_size():
+    v = ctypes.c_int()
+    check(lib().dfft_wisdom_size(ctypes.byref(v)))
     return v.value

@@ -135,10 +135,23 @@ DFFT_API int dfft_plan_destroy(dfft_plan plan);
 /*
  * Reads and clears the device error word of the current device.  Kernels
  * whose bounded waits expire (TMA tile pipeline) record a non-zero code there
- * instead of hanging: 1 = a tile load did not complete in time.  Synchronises
- * the device.
+ * instead of hanging or faulting: 1 = a tile load did not complete in time,
+ * 2 = a tile buffer was not aligned for the bulk copies (nothing was
+ * issued).  Synchronises the device.
  */
 DFFT_API int dfft_device_error(int* code);
+
+/*
+ * Tuning cache ("wisdom"; the reference imports FFTW wisdom at load and
+ * exports it after each new plan, src/fft.jl:113-124,162).  Plans created
+ * with DFFT_FLAG_TUNE time every launch candidate of each pass and record
+ * the fastest; later plans of the same pass shape reuse it.  The file format
+ * is text, one pass per line, keyed by the GPU model.
+ */
+DFFT_API int dfft_wisdom_export(const char* path);
+DFFT_API int dfft_wisdom_import(const char* path);
+DFFT_API int dfft_wisdom_forget(void);
+DFFT_API int dfft_wisdom_size(int* n);
 
 /* Thread-local description of the last error. */
 DFFT_API const char* dfft_last_error(void);

@@ -127,3 +127,29 @@ def test_unknown_transform_and_bad_args():
         dfft.fft(g, dims=(3,))
     with pytest.raises(dfft.ArgumentError, match="prime factor"):
         dfft.fft(torch.zeros((17 * 19,), dtype=torch.complex64, device="cuda"), dims=(1,))
+
+
+@pytest.mark.parametrize("shape", [(512, 64, 48), (64, 512, 8), (96, 96, 96), (256, 8, 512)])
+def test_tuned_plans_match(shape):
+    # DFFT_FLAG_TUNE times every launch candidate (pipelined / one-tile
+    # kernels, tile widths); whichever wins must give the same answer
+    a = rand(shape, np.complex64, seed=sum(shape))
+    g = to_gpu(a)
+    p = dfft.gpu_plan_transform(dfft.FFT(), g, (1, 2, 3), flags=dfft.FLAG_TUNE)
+    out = dfft.empty_like_layout(p.out_shape, g.dtype, g)
+    p.execute(g, out)
+    assert rel(to_np(out), oracle.fft(a, dims=(1, 2, 3))) <= 1e-5
+    assert dfft.wisdom_size() > 0
+    assert dfft.device_error() == 0
+
+
+def test_wisdom_roundtrip(tmp_path):
+    a = rand((64, 64, 64), np.complex64, seed=1)
+    dfft.gpu_plan_transform(dfft.FFT(), to_gpu(a), (1, 2, 3), flags=dfft.FLAG_TUNE)
+    n = dfft.wisdom_size()
+    f = tmp_path / "wisdom.txt"
+    dfft.wisdom_export(f)
+    dfft.wisdom_forget()
+    assert dfft.wisdom_size() == 0
+    dfft.wisdom_import(f)
+    assert dfft.wisdom_size() == n
