@@ -259,6 +259,13 @@ template <typename V> struct StrideCol {
   __device__ __forceinline__ V ld(int k) const { return p[k * s]; }
   __device__ __forceinline__ void st(int k, V v) const { p[k * s] = v; }
 };
+// StrideCol with a compile-time stride: every tile offset becomes an
+// immediate of the shared-memory instruction instead of a live register.
+template <typename V, int S> struct StrideColC {
+  V* p;
+  __device__ __forceinline__ V ld(int k) const { return p[k * S]; }
+  __device__ __forceinline__ void st(int k, V v) const { p[k * S] = v; }
+};
 
 // Twiddle sources.  GlobalTw reads w_L^{jm*r*ts} from the L-entry table;
 // StageTw reads a stage-major table laid out [stage][jm][r-1] (entry
@@ -275,6 +282,13 @@ template <typename V> struct StageTw {
   const V* p;
   __device__ __forceinline__ V w(int off, int jm, int r, int R, int ts) const {
     return p[off + jm * (R - 1) + r - 1];
+  }
+};
+// The same stage-major table read from global memory through L1.
+template <typename V> struct StageTwG {
+  const V* p;
+  __device__ __forceinline__ V w(int off, int jm, int r, int R, int ts) const {
+    return ldg_c(p + off + jm * (R - 1) + r - 1);
   }
 };
 

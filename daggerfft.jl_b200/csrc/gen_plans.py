@@ -89,6 +89,18 @@ def tma_bound(dt, lb):
     return min(lb, 512) if dt == "double" else lb
 
 
+def strided_c(dt, n, P, tlb):
+    """Columns per tile of the strided pipelined kernel (compile time): rows
+    of 128 bytes (16 complex float / 8 complex double), halved until three
+    tile buffers fit in shared memory and C*P threads fit the launch bound,
+    but never below 2 (16-byte TMA rows)."""
+    esz = 8 if dt == "float" else 16
+    C = 16 if dt == "float" else 8
+    while C > 2 and (C * P > tlb or 3 * C * n * esz + 128 > 227 * 1024):
+        C //= 2
+    return C
+
+
 def main():
     here = os.path.dirname(os.path.abspath(__file__))
     entries = []
@@ -115,8 +127,8 @@ def main():
                 lines.append(f"template __global__ void axis_pass_static<{dt},false,{lb},{n},{P},{rs}>(const PassDesc);")
                 if has_tma(dt, n):
                     tlb = tma_bound(dt, lb)
-                    for cg in ("false", "true"):
-                        lines.append(f"template __global__ void axis_pass_pipe<{dt},{tlb},{cg},{n},{P},{rs}>("
+                    for cg, cs in (("false", strided_c(dt, n, P, tlb)), ("true", 0)):
+                        lines.append(f"template __global__ void axis_pass_pipe<{dt},{tlb},{cg},{cs},{n},{P},{rs}>("
                                      "const PassDesc, const __grid_constant__ CUtensorMap, "
                                      "const __grid_constant__ CUtensorMap, const TmaGeom);")
             lines.append(f"extern const StaticPlan kPlans_{tag}_{fi}[];")
@@ -126,14 +138,16 @@ def main():
                 rs = ",".join(str(r) for r in rad)
                 radarr = "{" + ",".join(str(r) for r in rad) + "}"
                 tlb = tma_bound(dt, lb)
-                ps = (f"(const void*)&axis_pass_pipe<{dt},{tlb},false,{n},{P},{rs}>" if has_tma(dt, n)
+                cs = strided_c(dt, n, P, tlb)
+                ps = (f"(const void*)&axis_pass_pipe<{dt},{tlb},false,{cs},{n},{P},{rs}>" if has_tma(dt, n)
                       else "nullptr")
-                pc = (f"(const void*)&axis_pass_pipe<{dt},{tlb},true,{n},{P},{rs}>" if has_tma(dt, n)
+                pc = (f"(const void*)&axis_pass_pipe<{dt},{tlb},true,0,{n},{P},{rs}>" if has_tma(dt, n)
                       else "nullptr")
                 lines.append(
                     f"  {{{n}, {P}, {len(rad)}, {radarr}, {lb}, "
                     f"(const void*)&axis_pass_static<{dt},true,{lb},{n},{P},{rs}>, "
-                    f"(const void*)&axis_pass_static<{dt},false,{lb},{n},{P},{rs}>, {ps}, {pc}, {tlb}}},")
+                    f"(const void*)&axis_pass_static<{dt},false,{lb},{n},{P},{rs}>, {ps}, {pc}, {tlb}, "
+                    f"{cs if has_tma(dt, n) else 0}}},")
             lines.append("};")
             lines.append(f"const int kPlansCount_{tag}_{fi} = {len(ch)};")
             lines.append("}  // namespace dfft")

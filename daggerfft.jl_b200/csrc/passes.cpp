@@ -364,22 +364,25 @@ Pass make_pass(const PassSpec& s) {
     auto stw = stage_twiddles(s.dbl, L, rad);
     p.tables.push_back(stw);
     d.tw = stw->p;
+    auto twl = twiddle_table(s.dbl, L, 1, 0, L, false);
+    p.tables.push_back(twl);
+    d.tw2 = twl->p;
     TmaGeom& g = p.geom;
-    g.ntw = d.nst > 1 ? L - rad[0] : 0;
+    g.ntw = (contig && d.nst > 1) ? L - rad[0] : 0;
     const size_t tw_bytes = ((size_t)g.ntw * esz + 127) & ~(size_t)127;
     auto bstride_bytes = [&](int C) { return ((size_t)C * L * esz + 127) & ~(size_t)127; };
     auto smem_for = [&](int C) {
       return 128 + tw_bytes + (size_t)kTmaBufs * bstride_bytes(C) + (contig ? (size_t)C * ld * esz : 0);
     };
     int C = s.C;
-    if (C <= 0) {
-      if (contig) {
-        C = 1;
-        while (C * 2 * P <= 256 && smem_for(C * 2) <= smax) C *= 2;
-      } else {
-        C = s.dbl ? 8 : 16;
-        while (C * P < 256 && C < 64 && smem_for(C * 2) <= smax) C *= 2;
-      }
+    if (!contig) {
+      // the strided kernel has its tile width compiled in
+      if (C > 0 && C != sp->pipe_cs)
+        throw Error{DFFT_ERROR_INVALID_VALUE, "strided pipelined kernel has a fixed tile width"};
+      C = sp->pipe_cs;
+    } else if (C <= 0) {
+      C = 1;
+      while (C * 2 * P <= 256 && smem_for(C * 2) <= smax) C *= 2;
     }
     while (C > 1 && (C * P > lb || smem_for(C) > smax)) C /= 2;
     if (!contig && C % 2) C = 2;  // 16-byte TMA rows for complex float

@@ -5,60 +5,60 @@ template __global__ void axis_pass_static<float,true,1024,1,1,1>(const PassDesc)
 template __global__ void axis_pass_static<float,false,1024,1,1,1>(const PassDesc);
 template __global__ void axis_pass_static<float,true,1024,8,1,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,8,1,8>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,8,1,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,8,1,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,8,1,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,8,1,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,18,3,6,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,18,3,6,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,18,3,6,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,18,3,6,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,18,3,6,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,18,3,6,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,32,4,8,4>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,32,4,8,4>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,32,4,8,4>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,32,4,8,4>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,32,4,8,4>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,32,4,8,4>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,54,9,6,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,54,9,6,3,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,54,9,6,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,54,9,6,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,54,9,6,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,54,9,6,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,81,27,3,3,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,81,27,3,3,3,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,81,27,3,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,81,27,3,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,81,27,3,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,81,27,3,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,125,25,5,5,5>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,125,25,5,5,5>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,125,25,5,5,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,125,25,5,5,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,125,25,5,5,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,125,25,5,5,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,162,27,6,3,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,162,27,6,3,3,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,162,27,6,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,162,27,6,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,162,27,6,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,162,27,6,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,512,240,15,15,16>(const PassDesc);
 template __global__ void axis_pass_static<float,false,512,240,15,15,16>(const PassDesc);
-template __global__ void axis_pass_pipe<float,512,false,240,15,15,16>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,512,true,240,15,15,16>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,512,false,16,240,15,15,16>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,512,true,0,240,15,15,16>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,300,30,10,6,5>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,300,30,10,6,5>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,300,30,10,6,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,300,30,10,6,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,300,30,10,6,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,300,30,10,6,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,400,40,10,5,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,400,40,10,5,8>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,400,40,10,5,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,400,40,10,5,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,400,40,10,5,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,400,40,10,5,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,500,50,10,10,5>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,500,50,10,10,5>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,500,50,10,10,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,500,50,10,10,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,500,50,10,10,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,500,50,10,10,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,640,64,10,8,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,640,64,10,8,8>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,640,64,10,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,640,64,10,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,8,640,64,10,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,640,64,10,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,768,64,12,8,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,768,64,12,8,8>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,768,64,12,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,768,64,12,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,8,768,64,12,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,768,64,12,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,972,162,6,6,3,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,972,162,6,6,3,3,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,972,162,6,6,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,972,162,6,6,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,4,972,162,6,6,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,972,162,6,6,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,512,1200,100,12,10,10>(const PassDesc);
 template __global__ void axis_pass_static<float,false,512,1200,100,12,10,10>(const PassDesc);
 template __global__ void axis_pass_static<float,true,512,1440,120,12,12,10>(const PassDesc);
@@ -78,29 +78,29 @@ template __global__ void axis_pass_static<float,false,512,3840,240,15,16,16>(con
 extern const StaticPlan kPlans_f32_0[];
 extern const int kPlansCount_f32_0;
 const StaticPlan kPlans_f32_0[] = {
-  {1, 1, 1, {1}, 1024, (const void*)&axis_pass_static<float,true,1024,1,1,1>, (const void*)&axis_pass_static<float,false,1024,1,1,1>, nullptr, nullptr, 1024},
-  {8, 1, 1, {8}, 1024, (const void*)&axis_pass_static<float,true,1024,8,1,8>, (const void*)&axis_pass_static<float,false,1024,8,1,8>, (const void*)&axis_pass_pipe<float,1024,false,8,1,8>, (const void*)&axis_pass_pipe<float,1024,true,8,1,8>, 1024},
-  {18, 3, 2, {6,3}, 1024, (const void*)&axis_pass_static<float,true,1024,18,3,6,3>, (const void*)&axis_pass_static<float,false,1024,18,3,6,3>, (const void*)&axis_pass_pipe<float,1024,false,18,3,6,3>, (const void*)&axis_pass_pipe<float,1024,true,18,3,6,3>, 1024},
-  {32, 4, 2, {8,4}, 1024, (const void*)&axis_pass_static<float,true,1024,32,4,8,4>, (const void*)&axis_pass_static<float,false,1024,32,4,8,4>, (const void*)&axis_pass_pipe<float,1024,false,32,4,8,4>, (const void*)&axis_pass_pipe<float,1024,true,32,4,8,4>, 1024},
-  {54, 9, 3, {6,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,54,9,6,3,3>, (const void*)&axis_pass_static<float,false,1024,54,9,6,3,3>, (const void*)&axis_pass_pipe<float,1024,false,54,9,6,3,3>, (const void*)&axis_pass_pipe<float,1024,true,54,9,6,3,3>, 1024},
-  {81, 27, 4, {3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,81,27,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,81,27,3,3,3,3>, (const void*)&axis_pass_pipe<float,1024,false,81,27,3,3,3,3>, (const void*)&axis_pass_pipe<float,1024,true,81,27,3,3,3,3>, 1024},
-  {125, 25, 3, {5,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,125,25,5,5,5>, (const void*)&axis_pass_static<float,false,1024,125,25,5,5,5>, (const void*)&axis_pass_pipe<float,1024,false,125,25,5,5,5>, (const void*)&axis_pass_pipe<float,1024,true,125,25,5,5,5>, 1024},
-  {162, 27, 4, {6,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,162,27,6,3,3,3>, (const void*)&axis_pass_static<float,false,1024,162,27,6,3,3,3>, (const void*)&axis_pass_pipe<float,1024,false,162,27,6,3,3,3>, (const void*)&axis_pass_pipe<float,1024,true,162,27,6,3,3,3>, 1024},
-  {240, 15, 2, {15,16}, 512, (const void*)&axis_pass_static<float,true,512,240,15,15,16>, (const void*)&axis_pass_static<float,false,512,240,15,15,16>, (const void*)&axis_pass_pipe<float,512,false,240,15,15,16>, (const void*)&axis_pass_pipe<float,512,true,240,15,15,16>, 512},
-  {300, 30, 3, {10,6,5}, 1024, (const void*)&axis_pass_static<float,true,1024,300,30,10,6,5>, (const void*)&axis_pass_static<float,false,1024,300,30,10,6,5>, (const void*)&axis_pass_pipe<float,1024,false,300,30,10,6,5>, (const void*)&axis_pass_pipe<float,1024,true,300,30,10,6,5>, 1024},
-  {400, 40, 3, {10,5,8}, 1024, (const void*)&axis_pass_static<float,true,1024,400,40,10,5,8>, (const void*)&axis_pass_static<float,false,1024,400,40,10,5,8>, (const void*)&axis_pass_pipe<float,1024,false,400,40,10,5,8>, (const void*)&axis_pass_pipe<float,1024,true,400,40,10,5,8>, 1024},
-  {500, 50, 3, {10,10,5}, 1024, (const void*)&axis_pass_static<float,true,1024,500,50,10,10,5>, (const void*)&axis_pass_static<float,false,1024,500,50,10,10,5>, (const void*)&axis_pass_pipe<float,1024,false,500,50,10,10,5>, (const void*)&axis_pass_pipe<float,1024,true,500,50,10,10,5>, 1024},
-  {640, 64, 3, {10,8,8}, 1024, (const void*)&axis_pass_static<float,true,1024,640,64,10,8,8>, (const void*)&axis_pass_static<float,false,1024,640,64,10,8,8>, (const void*)&axis_pass_pipe<float,1024,false,640,64,10,8,8>, (const void*)&axis_pass_pipe<float,1024,true,640,64,10,8,8>, 1024},
-  {768, 64, 3, {12,8,8}, 1024, (const void*)&axis_pass_static<float,true,1024,768,64,12,8,8>, (const void*)&axis_pass_static<float,false,1024,768,64,12,8,8>, (const void*)&axis_pass_pipe<float,1024,false,768,64,12,8,8>, (const void*)&axis_pass_pipe<float,1024,true,768,64,12,8,8>, 1024},
-  {972, 162, 5, {6,6,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,972,162,6,6,3,3,3>, (const void*)&axis_pass_static<float,false,1024,972,162,6,6,3,3,3>, (const void*)&axis_pass_pipe<float,1024,false,972,162,6,6,3,3,3>, (const void*)&axis_pass_pipe<float,1024,true,972,162,6,6,3,3,3>, 1024},
-  {1200, 100, 3, {12,10,10}, 512, (const void*)&axis_pass_static<float,true,512,1200,100,12,10,10>, (const void*)&axis_pass_static<float,false,512,1200,100,12,10,10>, nullptr, nullptr, 512},
-  {1440, 120, 3, {12,12,10}, 512, (const void*)&axis_pass_static<float,true,512,1440,120,12,12,10>, (const void*)&axis_pass_static<float,false,512,1440,120,12,12,10>, nullptr, nullptr, 512},
-  {1728, 144, 3, {12,12,12}, 1024, (const void*)&axis_pass_static<float,true,1024,1728,144,12,12,12>, (const void*)&axis_pass_static<float,false,1024,1728,144,12,12,12>, nullptr, nullptr, 1024},
-  {2025, 135, 4, {15,15,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,2025,135,15,15,3,3>, (const void*)&axis_pass_static<float,false,1024,2025,135,15,15,3,3>, nullptr, nullptr, 1024},
-  {2400, 150, 3, {15,10,16}, 512, (const void*)&axis_pass_static<float,true,512,2400,150,15,10,16>, (const void*)&axis_pass_static<float,false,512,2400,150,15,10,16>, nullptr, nullptr, 512},
-  {2880, 180, 3, {15,12,16}, 512, (const void*)&axis_pass_static<float,true,512,2880,180,15,12,16>, (const void*)&axis_pass_static<float,false,512,2880,180,15,12,16>, nullptr, nullptr, 512},
-  {3240, 216, 4, {15,6,6,6}, 512, (const void*)&axis_pass_static<float,true,512,3240,216,15,6,6,6>, (const void*)&axis_pass_static<float,false,512,3240,216,15,6,6,6>, nullptr, nullptr, 512},
-  {3840, 240, 3, {15,16,16}, 512, (const void*)&axis_pass_static<float,true,512,3840,240,15,16,16>, (const void*)&axis_pass_static<float,false,512,3840,240,15,16,16>, nullptr, nullptr, 512},
+  {1, 1, 1, {1}, 1024, (const void*)&axis_pass_static<float,true,1024,1,1,1>, (const void*)&axis_pass_static<float,false,1024,1,1,1>, nullptr, nullptr, 1024, 0},
+  {8, 1, 1, {8}, 1024, (const void*)&axis_pass_static<float,true,1024,8,1,8>, (const void*)&axis_pass_static<float,false,1024,8,1,8>, (const void*)&axis_pass_pipe<float,1024,false,16,8,1,8>, (const void*)&axis_pass_pipe<float,1024,true,0,8,1,8>, 1024, 16},
+  {18, 3, 2, {6,3}, 1024, (const void*)&axis_pass_static<float,true,1024,18,3,6,3>, (const void*)&axis_pass_static<float,false,1024,18,3,6,3>, (const void*)&axis_pass_pipe<float,1024,false,16,18,3,6,3>, (const void*)&axis_pass_pipe<float,1024,true,0,18,3,6,3>, 1024, 16},
+  {32, 4, 2, {8,4}, 1024, (const void*)&axis_pass_static<float,true,1024,32,4,8,4>, (const void*)&axis_pass_static<float,false,1024,32,4,8,4>, (const void*)&axis_pass_pipe<float,1024,false,16,32,4,8,4>, (const void*)&axis_pass_pipe<float,1024,true,0,32,4,8,4>, 1024, 16},
+  {54, 9, 3, {6,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,54,9,6,3,3>, (const void*)&axis_pass_static<float,false,1024,54,9,6,3,3>, (const void*)&axis_pass_pipe<float,1024,false,16,54,9,6,3,3>, (const void*)&axis_pass_pipe<float,1024,true,0,54,9,6,3,3>, 1024, 16},
+  {81, 27, 4, {3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,81,27,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,81,27,3,3,3,3>, (const void*)&axis_pass_pipe<float,1024,false,16,81,27,3,3,3,3>, (const void*)&axis_pass_pipe<float,1024,true,0,81,27,3,3,3,3>, 1024, 16},
+  {125, 25, 3, {5,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,125,25,5,5,5>, (const void*)&axis_pass_static<float,false,1024,125,25,5,5,5>, (const void*)&axis_pass_pipe<float,1024,false,16,125,25,5,5,5>, (const void*)&axis_pass_pipe<float,1024,true,0,125,25,5,5,5>, 1024, 16},
+  {162, 27, 4, {6,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,162,27,6,3,3,3>, (const void*)&axis_pass_static<float,false,1024,162,27,6,3,3,3>, (const void*)&axis_pass_pipe<float,1024,false,16,162,27,6,3,3,3>, (const void*)&axis_pass_pipe<float,1024,true,0,162,27,6,3,3,3>, 1024, 16},
+  {240, 15, 2, {15,16}, 512, (const void*)&axis_pass_static<float,true,512,240,15,15,16>, (const void*)&axis_pass_static<float,false,512,240,15,15,16>, (const void*)&axis_pass_pipe<float,512,false,16,240,15,15,16>, (const void*)&axis_pass_pipe<float,512,true,0,240,15,15,16>, 512, 16},
+  {300, 30, 3, {10,6,5}, 1024, (const void*)&axis_pass_static<float,true,1024,300,30,10,6,5>, (const void*)&axis_pass_static<float,false,1024,300,30,10,6,5>, (const void*)&axis_pass_pipe<float,1024,false,16,300,30,10,6,5>, (const void*)&axis_pass_pipe<float,1024,true,0,300,30,10,6,5>, 1024, 16},
+  {400, 40, 3, {10,5,8}, 1024, (const void*)&axis_pass_static<float,true,1024,400,40,10,5,8>, (const void*)&axis_pass_static<float,false,1024,400,40,10,5,8>, (const void*)&axis_pass_pipe<float,1024,false,16,400,40,10,5,8>, (const void*)&axis_pass_pipe<float,1024,true,0,400,40,10,5,8>, 1024, 16},
+  {500, 50, 3, {10,10,5}, 1024, (const void*)&axis_pass_static<float,true,1024,500,50,10,10,5>, (const void*)&axis_pass_static<float,false,1024,500,50,10,10,5>, (const void*)&axis_pass_pipe<float,1024,false,16,500,50,10,10,5>, (const void*)&axis_pass_pipe<float,1024,true,0,500,50,10,10,5>, 1024, 16},
+  {640, 64, 3, {10,8,8}, 1024, (const void*)&axis_pass_static<float,true,1024,640,64,10,8,8>, (const void*)&axis_pass_static<float,false,1024,640,64,10,8,8>, (const void*)&axis_pass_pipe<float,1024,false,8,640,64,10,8,8>, (const void*)&axis_pass_pipe<float,1024,true,0,640,64,10,8,8>, 1024, 8},
+  {768, 64, 3, {12,8,8}, 1024, (const void*)&axis_pass_static<float,true,1024,768,64,12,8,8>, (const void*)&axis_pass_static<float,false,1024,768,64,12,8,8>, (const void*)&axis_pass_pipe<float,1024,false,8,768,64,12,8,8>, (const void*)&axis_pass_pipe<float,1024,true,0,768,64,12,8,8>, 1024, 8},
+  {972, 162, 5, {6,6,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,972,162,6,6,3,3,3>, (const void*)&axis_pass_static<float,false,1024,972,162,6,6,3,3,3>, (const void*)&axis_pass_pipe<float,1024,false,4,972,162,6,6,3,3,3>, (const void*)&axis_pass_pipe<float,1024,true,0,972,162,6,6,3,3,3>, 1024, 4},
+  {1200, 100, 3, {12,10,10}, 512, (const void*)&axis_pass_static<float,true,512,1200,100,12,10,10>, (const void*)&axis_pass_static<float,false,512,1200,100,12,10,10>, nullptr, nullptr, 512, 0},
+  {1440, 120, 3, {12,12,10}, 512, (const void*)&axis_pass_static<float,true,512,1440,120,12,12,10>, (const void*)&axis_pass_static<float,false,512,1440,120,12,12,10>, nullptr, nullptr, 512, 0},
+  {1728, 144, 3, {12,12,12}, 1024, (const void*)&axis_pass_static<float,true,1024,1728,144,12,12,12>, (const void*)&axis_pass_static<float,false,1024,1728,144,12,12,12>, nullptr, nullptr, 1024, 0},
+  {2025, 135, 4, {15,15,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,2025,135,15,15,3,3>, (const void*)&axis_pass_static<float,false,1024,2025,135,15,15,3,3>, nullptr, nullptr, 1024, 0},
+  {2400, 150, 3, {15,10,16}, 512, (const void*)&axis_pass_static<float,true,512,2400,150,15,10,16>, (const void*)&axis_pass_static<float,false,512,2400,150,15,10,16>, nullptr, nullptr, 512, 0},
+  {2880, 180, 3, {15,12,16}, 512, (const void*)&axis_pass_static<float,true,512,2880,180,15,12,16>, (const void*)&axis_pass_static<float,false,512,2880,180,15,12,16>, nullptr, nullptr, 512, 0},
+  {3240, 216, 4, {15,6,6,6}, 512, (const void*)&axis_pass_static<float,true,512,3240,216,15,6,6,6>, (const void*)&axis_pass_static<float,false,512,3240,216,15,6,6,6>, nullptr, nullptr, 512, 0},
+  {3840, 240, 3, {15,16,16}, 512, (const void*)&axis_pass_static<float,true,512,3840,240,15,16,16>, (const void*)&axis_pass_static<float,false,512,3840,240,15,16,16>, nullptr, nullptr, 512, 0},
 };
 const int kPlansCount_f32_0 = 23;
 }  // namespace dfft

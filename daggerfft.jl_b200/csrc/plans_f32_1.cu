@@ -5,60 +5,60 @@ template __global__ void axis_pass_static<float,true,1024,2,1,2>(const PassDesc)
 template __global__ void axis_pass_static<float,false,1024,2,1,2>(const PassDesc);
 template __global__ void axis_pass_static<float,true,1024,9,3,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,9,3,3,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,9,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,9,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,9,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,9,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,20,4,5,4>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,20,4,5,4>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,20,4,5,4>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,20,4,5,4>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,20,4,5,4>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,20,4,5,4>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,36,6,6,6>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,36,6,6,6>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,36,6,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,36,6,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,36,6,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,36,6,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,60,6,10,6>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,60,6,10,6>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,60,6,10,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,60,6,10,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,60,6,10,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,60,6,10,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,512,90,6,15,6>(const PassDesc);
 template __global__ void axis_pass_static<float,false,512,90,6,15,6>(const PassDesc);
-template __global__ void axis_pass_pipe<float,512,false,90,6,15,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,512,true,90,6,15,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,512,false,16,90,6,15,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,512,true,0,90,6,15,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,128,8,16,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,128,8,16,8>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,128,8,16,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,128,8,16,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,128,8,16,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,128,8,16,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,512,180,12,15,12>(const PassDesc);
 template __global__ void axis_pass_static<float,false,512,180,12,15,12>(const PassDesc);
-template __global__ void axis_pass_pipe<float,512,false,180,12,15,12>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,512,true,180,12,15,12>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,512,false,16,180,12,15,12>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,512,true,0,180,12,15,12>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,243,81,3,3,3,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,243,81,3,3,3,3,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,243,81,3,3,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,243,81,3,3,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,8,243,81,3,3,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,243,81,3,3,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,320,40,5,8,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,320,40,5,8,8>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,320,40,5,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,320,40,5,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,320,40,5,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,320,40,5,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,405,27,15,3,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,405,27,15,3,3,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,405,27,15,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,405,27,15,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,405,27,15,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,405,27,15,3,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,512,64,8,8,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,512,64,8,8,8>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,512,64,8,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,512,64,8,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,512,64,8,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,512,64,8,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,648,108,6,6,6,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,648,108,6,6,6,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,648,108,6,6,6,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,648,108,6,6,6,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,8,648,108,6,6,6,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,648,108,6,6,6,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,800,80,10,10,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,800,80,10,10,8>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,800,80,10,10,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,800,80,10,10,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,8,800,80,10,10,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,800,80,10,10,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,1000,100,10,10,10>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,1000,100,10,10,10>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,1000,100,10,10,10>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,1000,100,10,10,10>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,8,1000,100,10,10,10>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,1000,100,10,10,10>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,1215,81,15,3,3,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,1215,81,15,3,3,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,true,1024,1458,243,6,3,3,3,3,3>(const PassDesc);
@@ -78,29 +78,29 @@ template __global__ void axis_pass_static<float,false,1024,3888,648,6,6,6,6,3>(c
 extern const StaticPlan kPlans_f32_1[];
 extern const int kPlansCount_f32_1;
 const StaticPlan kPlans_f32_1[] = {
-  {2, 1, 1, {2}, 1024, (const void*)&axis_pass_static<float,true,1024,2,1,2>, (const void*)&axis_pass_static<float,false,1024,2,1,2>, nullptr, nullptr, 1024},
-  {9, 3, 2, {3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,9,3,3,3>, (const void*)&axis_pass_static<float,false,1024,9,3,3,3>, (const void*)&axis_pass_pipe<float,1024,false,9,3,3,3>, (const void*)&axis_pass_pipe<float,1024,true,9,3,3,3>, 1024},
-  {20, 4, 2, {5,4}, 1024, (const void*)&axis_pass_static<float,true,1024,20,4,5,4>, (const void*)&axis_pass_static<float,false,1024,20,4,5,4>, (const void*)&axis_pass_pipe<float,1024,false,20,4,5,4>, (const void*)&axis_pass_pipe<float,1024,true,20,4,5,4>, 1024},
-  {36, 6, 2, {6,6}, 1024, (const void*)&axis_pass_static<float,true,1024,36,6,6,6>, (const void*)&axis_pass_static<float,false,1024,36,6,6,6>, (const void*)&axis_pass_pipe<float,1024,false,36,6,6,6>, (const void*)&axis_pass_pipe<float,1024,true,36,6,6,6>, 1024},
-  {60, 6, 2, {10,6}, 1024, (const void*)&axis_pass_static<float,true,1024,60,6,10,6>, (const void*)&axis_pass_static<float,false,1024,60,6,10,6>, (const void*)&axis_pass_pipe<float,1024,false,60,6,10,6>, (const void*)&axis_pass_pipe<float,1024,true,60,6,10,6>, 1024},
-  {90, 6, 2, {15,6}, 512, (const void*)&axis_pass_static<float,true,512,90,6,15,6>, (const void*)&axis_pass_static<float,false,512,90,6,15,6>, (const void*)&axis_pass_pipe<float,512,false,90,6,15,6>, (const void*)&axis_pass_pipe<float,512,true,90,6,15,6>, 512},
-  {128, 8, 2, {16,8}, 1024, (const void*)&axis_pass_static<float,true,1024,128,8,16,8>, (const void*)&axis_pass_static<float,false,1024,128,8,16,8>, (const void*)&axis_pass_pipe<float,1024,false,128,8,16,8>, (const void*)&axis_pass_pipe<float,1024,true,128,8,16,8>, 1024},
-  {180, 12, 2, {15,12}, 512, (const void*)&axis_pass_static<float,true,512,180,12,15,12>, (const void*)&axis_pass_static<float,false,512,180,12,15,12>, (const void*)&axis_pass_pipe<float,512,false,180,12,15,12>, (const void*)&axis_pass_pipe<float,512,true,180,12,15,12>, 512},
-  {243, 81, 5, {3,3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,243,81,3,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,243,81,3,3,3,3,3>, (const void*)&axis_pass_pipe<float,1024,false,243,81,3,3,3,3,3>, (const void*)&axis_pass_pipe<float,1024,true,243,81,3,3,3,3,3>, 1024},
-  {320, 40, 3, {5,8,8}, 1024, (const void*)&axis_pass_static<float,true,1024,320,40,5,8,8>, (const void*)&axis_pass_static<float,false,1024,320,40,5,8,8>, (const void*)&axis_pass_pipe<float,1024,false,320,40,5,8,8>, (const void*)&axis_pass_pipe<float,1024,true,320,40,5,8,8>, 1024},
-  {405, 27, 4, {15,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,405,27,15,3,3,3>, (const void*)&axis_pass_static<float,false,1024,405,27,15,3,3,3>, (const void*)&axis_pass_pipe<float,1024,false,405,27,15,3,3,3>, (const void*)&axis_pass_pipe<float,1024,true,405,27,15,3,3,3>, 1024},
-  {512, 64, 3, {8,8,8}, 1024, (const void*)&axis_pass_static<float,true,1024,512,64,8,8,8>, (const void*)&axis_pass_static<float,false,1024,512,64,8,8,8>, (const void*)&axis_pass_pipe<float,1024,false,512,64,8,8,8>, (const void*)&axis_pass_pipe<float,1024,true,512,64,8,8,8>, 1024},
-  {648, 108, 4, {6,6,6,3}, 1024, (const void*)&axis_pass_static<float,true,1024,648,108,6,6,6,3>, (const void*)&axis_pass_static<float,false,1024,648,108,6,6,6,3>, (const void*)&axis_pass_pipe<float,1024,false,648,108,6,6,6,3>, (const void*)&axis_pass_pipe<float,1024,true,648,108,6,6,6,3>, 1024},
-  {800, 80, 3, {10,10,8}, 1024, (const void*)&axis_pass_static<float,true,1024,800,80,10,10,8>, (const void*)&axis_pass_static<float,false,1024,800,80,10,10,8>, (const void*)&axis_pass_pipe<float,1024,false,800,80,10,10,8>, (const void*)&axis_pass_pipe<float,1024,true,800,80,10,10,8>, 1024},
-  {1000, 100, 3, {10,10,10}, 1024, (const void*)&axis_pass_static<float,true,1024,1000,100,10,10,10>, (const void*)&axis_pass_static<float,false,1024,1000,100,10,10,10>, (const void*)&axis_pass_pipe<float,1024,false,1000,100,10,10,10>, (const void*)&axis_pass_pipe<float,1024,true,1000,100,10,10,10>, 1024},
-  {1215, 81, 5, {15,3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,1215,81,15,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,1215,81,15,3,3,3,3>, nullptr, nullptr, 1024},
-  {1458, 243, 6, {6,3,3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,1458,243,6,3,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,1458,243,6,3,3,3,3,3>, nullptr, nullptr, 1024},
-  {1800, 120, 3, {15,12,10}, 512, (const void*)&axis_pass_static<float,true,512,1800,120,15,12,10>, (const void*)&axis_pass_static<float,false,512,1800,120,15,12,10>, nullptr, nullptr, 512},
-  {2048, 128, 3, {16,16,8}, 1024, (const void*)&axis_pass_static<float,true,1024,2048,128,16,16,8>, (const void*)&axis_pass_static<float,false,1024,2048,128,16,16,8>, nullptr, nullptr, 1024},
-  {2430, 162, 5, {15,6,3,3,3}, 512, (const void*)&axis_pass_static<float,true,512,2430,162,15,6,3,3,3>, (const void*)&axis_pass_static<float,false,512,2430,162,15,6,3,3,3>, nullptr, nullptr, 512},
-  {2916, 486, 6, {6,6,3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,2916,486,6,6,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,2916,486,6,6,3,3,3,3>, nullptr, nullptr, 1024},
-  {3375, 225, 3, {15,15,15}, 1024, (const void*)&axis_pass_static<float,true,1024,3375,225,15,15,15>, (const void*)&axis_pass_static<float,false,1024,3375,225,15,15,15>, nullptr, nullptr, 1024},
-  {3888, 648, 5, {6,6,6,6,3}, 1024, (const void*)&axis_pass_static<float,true,1024,3888,648,6,6,6,6,3>, (const void*)&axis_pass_static<float,false,1024,3888,648,6,6,6,6,3>, nullptr, nullptr, 1024},
+  {2, 1, 1, {2}, 1024, (const void*)&axis_pass_static<float,true,1024,2,1,2>, (const void*)&axis_pass_static<float,false,1024,2,1,2>, nullptr, nullptr, 1024, 0},
+  {9, 3, 2, {3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,9,3,3,3>, (const void*)&axis_pass_static<float,false,1024,9,3,3,3>, (const void*)&axis_pass_pipe<float,1024,false,16,9,3,3,3>, (const void*)&axis_pass_pipe<float,1024,true,0,9,3,3,3>, 1024, 16},
+  {20, 4, 2, {5,4}, 1024, (const void*)&axis_pass_static<float,true,1024,20,4,5,4>, (const void*)&axis_pass_static<float,false,1024,20,4,5,4>, (const void*)&axis_pass_pipe<float,1024,false,16,20,4,5,4>, (const void*)&axis_pass_pipe<float,1024,true,0,20,4,5,4>, 1024, 16},
+  {36, 6, 2, {6,6}, 1024, (const void*)&axis_pass_static<float,true,1024,36,6,6,6>, (const void*)&axis_pass_static<float,false,1024,36,6,6,6>, (const void*)&axis_pass_pipe<float,1024,false,16,36,6,6,6>, (const void*)&axis_pass_pipe<float,1024,true,0,36,6,6,6>, 1024, 16},
+  {60, 6, 2, {10,6}, 1024, (const void*)&axis_pass_static<float,true,1024,60,6,10,6>, (const void*)&axis_pass_static<float,false,1024,60,6,10,6>, (const void*)&axis_pass_pipe<float,1024,false,16,60,6,10,6>, (const void*)&axis_pass_pipe<float,1024,true,0,60,6,10,6>, 1024, 16},
+  {90, 6, 2, {15,6}, 512, (const void*)&axis_pass_static<float,true,512,90,6,15,6>, (const void*)&axis_pass_static<float,false,512,90,6,15,6>, (const void*)&axis_pass_pipe<float,512,false,16,90,6,15,6>, (const void*)&axis_pass_pipe<float,512,true,0,90,6,15,6>, 512, 16},
+  {128, 8, 2, {16,8}, 1024, (const void*)&axis_pass_static<float,true,1024,128,8,16,8>, (const void*)&axis_pass_static<float,false,1024,128,8,16,8>, (const void*)&axis_pass_pipe<float,1024,false,16,128,8,16,8>, (const void*)&axis_pass_pipe<float,1024,true,0,128,8,16,8>, 1024, 16},
+  {180, 12, 2, {15,12}, 512, (const void*)&axis_pass_static<float,true,512,180,12,15,12>, (const void*)&axis_pass_static<float,false,512,180,12,15,12>, (const void*)&axis_pass_pipe<float,512,false,16,180,12,15,12>, (const void*)&axis_pass_pipe<float,512,true,0,180,12,15,12>, 512, 16},
+  {243, 81, 5, {3,3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,243,81,3,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,243,81,3,3,3,3,3>, (const void*)&axis_pass_pipe<float,1024,false,8,243,81,3,3,3,3,3>, (const void*)&axis_pass_pipe<float,1024,true,0,243,81,3,3,3,3,3>, 1024, 8},
+  {320, 40, 3, {5,8,8}, 1024, (const void*)&axis_pass_static<float,true,1024,320,40,5,8,8>, (const void*)&axis_pass_static<float,false,1024,320,40,5,8,8>, (const void*)&axis_pass_pipe<float,1024,false,16,320,40,5,8,8>, (const void*)&axis_pass_pipe<float,1024,true,0,320,40,5,8,8>, 1024, 16},
+  {405, 27, 4, {15,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,405,27,15,3,3,3>, (const void*)&axis_pass_static<float,false,1024,405,27,15,3,3,3>, (const void*)&axis_pass_pipe<float,1024,false,16,405,27,15,3,3,3>, (const void*)&axis_pass_pipe<float,1024,true,0,405,27,15,3,3,3>, 1024, 16},
+  {512, 64, 3, {8,8,8}, 1024, (const void*)&axis_pass_static<float,true,1024,512,64,8,8,8>, (const void*)&axis_pass_static<float,false,1024,512,64,8,8,8>, (const void*)&axis_pass_pipe<float,1024,false,16,512,64,8,8,8>, (const void*)&axis_pass_pipe<float,1024,true,0,512,64,8,8,8>, 1024, 16},
+  {648, 108, 4, {6,6,6,3}, 1024, (const void*)&axis_pass_static<float,true,1024,648,108,6,6,6,3>, (const void*)&axis_pass_static<float,false,1024,648,108,6,6,6,3>, (const void*)&axis_pass_pipe<float,1024,false,8,648,108,6,6,6,3>, (const void*)&axis_pass_pipe<float,1024,true,0,648,108,6,6,6,3>, 1024, 8},
+  {800, 80, 3, {10,10,8}, 1024, (const void*)&axis_pass_static<float,true,1024,800,80,10,10,8>, (const void*)&axis_pass_static<float,false,1024,800,80,10,10,8>, (const void*)&axis_pass_pipe<float,1024,false,8,800,80,10,10,8>, (const void*)&axis_pass_pipe<float,1024,true,0,800,80,10,10,8>, 1024, 8},
+  {1000, 100, 3, {10,10,10}, 1024, (const void*)&axis_pass_static<float,true,1024,1000,100,10,10,10>, (const void*)&axis_pass_static<float,false,1024,1000,100,10,10,10>, (const void*)&axis_pass_pipe<float,1024,false,8,1000,100,10,10,10>, (const void*)&axis_pass_pipe<float,1024,true,0,1000,100,10,10,10>, 1024, 8},
+  {1215, 81, 5, {15,3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,1215,81,15,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,1215,81,15,3,3,3,3>, nullptr, nullptr, 1024, 0},
+  {1458, 243, 6, {6,3,3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,1458,243,6,3,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,1458,243,6,3,3,3,3,3>, nullptr, nullptr, 1024, 0},
+  {1800, 120, 3, {15,12,10}, 512, (const void*)&axis_pass_static<float,true,512,1800,120,15,12,10>, (const void*)&axis_pass_static<float,false,512,1800,120,15,12,10>, nullptr, nullptr, 512, 0},
+  {2048, 128, 3, {16,16,8}, 1024, (const void*)&axis_pass_static<float,true,1024,2048,128,16,16,8>, (const void*)&axis_pass_static<float,false,1024,2048,128,16,16,8>, nullptr, nullptr, 1024, 0},
+  {2430, 162, 5, {15,6,3,3,3}, 512, (const void*)&axis_pass_static<float,true,512,2430,162,15,6,3,3,3>, (const void*)&axis_pass_static<float,false,512,2430,162,15,6,3,3,3>, nullptr, nullptr, 512, 0},
+  {2916, 486, 6, {6,6,3,3,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,2916,486,6,6,3,3,3,3>, (const void*)&axis_pass_static<float,false,1024,2916,486,6,6,3,3,3,3>, nullptr, nullptr, 1024, 0},
+  {3375, 225, 3, {15,15,15}, 1024, (const void*)&axis_pass_static<float,true,1024,3375,225,15,15,15>, (const void*)&axis_pass_static<float,false,1024,3375,225,15,15,15>, nullptr, nullptr, 1024, 0},
+  {3888, 648, 5, {6,6,6,6,3}, 1024, (const void*)&axis_pass_static<float,true,1024,3888,648,6,6,6,6,3>, (const void*)&axis_pass_static<float,false,1024,3888,648,6,6,6,6,3>, nullptr, nullptr, 1024, 0},
 };
 const int kPlansCount_f32_1 = 23;
 }  // namespace dfft

@@ -5,60 +5,60 @@ template __global__ void axis_pass_static<float,true,1024,3,1,3>(const PassDesc)
 template __global__ void axis_pass_static<float,false,1024,3,1,3>(const PassDesc);
 template __global__ void axis_pass_static<float,true,1024,10,1,10>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,10,1,10>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,10,1,10>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,10,1,10>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,10,1,10>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,10,1,10>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,24,4,6,4>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,24,4,6,4>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,24,4,6,4>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,24,4,6,4>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,24,4,6,4>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,24,4,6,4>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,40,5,5,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,40,5,5,8>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,40,5,5,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,40,5,5,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,40,5,5,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,40,5,5,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,64,8,8,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,64,8,8,8>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,64,8,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,64,8,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,64,8,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,64,8,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,96,8,12,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,96,8,12,8>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,96,8,12,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,96,8,12,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,96,8,12,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,96,8,12,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,135,9,15,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,135,9,15,3,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,135,9,15,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,135,9,15,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,135,9,15,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,135,9,15,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,512,192,12,12,16>(const PassDesc);
 template __global__ void axis_pass_static<float,false,512,192,12,12,16>(const PassDesc);
-template __global__ void axis_pass_pipe<float,512,false,192,12,12,16>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,512,true,192,12,12,16>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,512,false,16,192,12,12,16>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,512,true,0,192,12,12,16>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,250,25,10,5,5>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,250,25,10,5,5>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,250,25,10,5,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,250,25,10,5,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,250,25,10,5,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,250,25,10,5,5>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,324,54,6,6,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,324,54,6,6,3,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,324,54,6,6,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,324,54,6,6,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,324,54,6,6,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,324,54,6,6,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,432,36,12,6,6>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,432,36,12,6,6>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,432,36,12,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,432,36,12,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,16,432,36,12,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,432,36,12,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,512,540,36,15,6,6>(const PassDesc);
 template __global__ void axis_pass_static<float,false,512,540,36,15,6,6>(const PassDesc);
-template __global__ void axis_pass_pipe<float,512,false,540,36,15,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,512,true,540,36,15,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,512,false,8,540,36,15,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,512,true,0,540,36,15,6,6>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,675,45,15,15,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,675,45,15,15,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,675,45,15,15,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,675,45,15,15,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,8,675,45,15,15,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,675,45,15,15,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,512,810,54,15,6,3,3>(const PassDesc);
 template __global__ void axis_pass_static<float,false,512,810,54,15,6,3,3>(const PassDesc);
-template __global__ void axis_pass_pipe<float,512,false,810,54,15,6,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,512,true,810,54,15,6,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,512,false,8,810,54,15,6,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,512,true,0,810,54,15,6,3,3>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,1024,64,16,8,8>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,1024,64,16,8,8>(const PassDesc);
-template __global__ void axis_pass_pipe<float,1024,false,1024,64,16,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
-template __global__ void axis_pass_pipe<float,1024,true,1024,64,16,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,false,8,1024,64,16,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
+template __global__ void axis_pass_pipe<float,1024,true,0,1024,64,16,8,8>(const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap, const TmaGeom);
 template __global__ void axis_pass_static<float,true,1024,1250,125,10,5,5,5>(const PassDesc);
 template __global__ void axis_pass_static<float,false,1024,1250,125,10,5,5,5>(const PassDesc);
 template __global__ void axis_pass_static<float,true,512,1500,100,15,10,10>(const PassDesc);
@@ -78,29 +78,29 @@ template __global__ void axis_pass_static<float,false,1024,4000,400,10,10,5,8>(c
 extern const StaticPlan kPlans_f32_2[];
 extern const int kPlansCount_f32_2;
 const StaticPlan kPlans_f32_2[] = {
-  {3, 1, 1, {3}, 1024, (const void*)&axis_pass_static<float,true,1024,3,1,3>, (const void*)&axis_pass_static<float,false,1024,3,1,3>, nullptr, nullptr, 1024},
-  {10, 1, 1, {10}, 1024, (const void*)&axis_pass_static<float,true,1024,10,1,10>, (const void*)&axis_pass_static<float,false,1024,10,1,10>, (const void*)&axis_pass_pipe<float,1024,false,10,1,10>, (const void*)&axis_pass_pipe<float,1024,true,10,1,10>, 1024},
-  {24, 4, 2, {6,4}, 1024, (const void*)&axis_pass_static<float,true,1024,24,4,6,4>, (const void*)&axis_pass_static<float,false,1024,24,4,6,4>, (const void*)&axis_pass_pipe<float,1024,false,24,4,6,4>, (const void*)&axis_pass_pipe<float,1024,true,24,4,6,4>, 1024},
-  {40, 5, 2, {5,8}, 1024, (const void*)&axis_pass_static<float,true,1024,40,5,5,8>, (const void*)&axis_pass_static<float,false,1024,40,5,5,8>, (const void*)&axis_pass_pipe<float,1024,false,40,5,5,8>, (const void*)&axis_pass_pipe<float,1024,true,40,5,5,8>, 1024},
-  {64, 8, 2, {8,8}, 1024, (const void*)&axis_pass_static<float,true,1024,64,8,8,8>, (const void*)&axis_pass_static<float,false,1024,64,8,8,8>, (const void*)&axis_pass_pipe<float,1024,false,64,8,8,8>, (const void*)&axis_pass_pipe<float,1024,true,64,8,8,8>, 1024},
-  {96, 8, 2, {12,8}, 1024, (const void*)&axis_pass_static<float,true,1024,96,8,12,8>, (const void*)&axis_pass_static<float,false,1024,96,8,12,8>, (const void*)&axis_pass_pipe<float,1024,false,96,8,12,8>, (const void*)&axis_pass_pipe<float,1024,true,96,8,12,8>, 1024},
-  {135, 9, 3, {15,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,135,9,15,3,3>, (const void*)&axis_pass_static<float,false,1024,135,9,15,3,3>, (const void*)&axis_pass_pipe<float,1024,false,135,9,15,3,3>, (const void*)&axis_pass_pipe<float,1024,true,135,9,15,3,3>, 1024},
-  {192, 12, 2, {12,16}, 512, (const void*)&axis_pass_static<float,true,512,192,12,12,16>, (const void*)&axis_pass_static<float,false,512,192,12,12,16>, (const void*)&axis_pass_pipe<float,512,false,192,12,12,16>, (const void*)&axis_pass_pipe<float,512,true,192,12,12,16>, 512},
-  {250, 25, 3, {10,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,250,25,10,5,5>, (const void*)&axis_pass_static<float,false,1024,250,25,10,5,5>, (const void*)&axis_pass_pipe<float,1024,false,250,25,10,5,5>, (const void*)&axis_pass_pipe<float,1024,true,250,25,10,5,5>, 1024},
-  {324, 54, 4, {6,6,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,324,54,6,6,3,3>, (const void*)&axis_pass_static<float,false,1024,324,54,6,6,3,3>, (const void*)&axis_pass_pipe<float,1024,false,324,54,6,6,3,3>, (const void*)&axis_pass_pipe<float,1024,true,324,54,6,6,3,3>, 1024},
-  {432, 36, 3, {12,6,6}, 1024, (const void*)&axis_pass_static<float,true,1024,432,36,12,6,6>, (const void*)&axis_pass_static<float,false,1024,432,36,12,6,6>, (const void*)&axis_pass_pipe<float,1024,false,432,36,12,6,6>, (const void*)&axis_pass_pipe<float,1024,true,432,36,12,6,6>, 1024},
-  {540, 36, 3, {15,6,6}, 512, (const void*)&axis_pass_static<float,true,512,540,36,15,6,6>, (const void*)&axis_pass_static<float,false,512,540,36,15,6,6>, (const void*)&axis_pass_pipe<float,512,false,540,36,15,6,6>, (const void*)&axis_pass_pipe<float,512,true,540,36,15,6,6>, 512},
-  {675, 45, 3, {15,15,3}, 1024, (const void*)&axis_pass_static<float,true,1024,675,45,15,15,3>, (const void*)&axis_pass_static<float,false,1024,675,45,15,15,3>, (const void*)&axis_pass_pipe<float,1024,false,675,45,15,15,3>, (const void*)&axis_pass_pipe<float,1024,true,675,45,15,15,3>, 1024},
-  {810, 54, 4, {15,6,3,3}, 512, (const void*)&axis_pass_static<float,true,512,810,54,15,6,3,3>, (const void*)&axis_pass_static<float,false,512,810,54,15,6,3,3>, (const void*)&axis_pass_pipe<float,512,false,810,54,15,6,3,3>, (const void*)&axis_pass_pipe<float,512,true,810,54,15,6,3,3>, 512},
-  {1024, 64, 3, {16,8,8}, 1024, (const void*)&axis_pass_static<float,true,1024,1024,64,16,8,8>, (const void*)&axis_pass_static<float,false,1024,1024,64,16,8,8>, (const void*)&axis_pass_pipe<float,1024,false,1024,64,16,8,8>, (const void*)&axis_pass_pipe<float,1024,true,1024,64,16,8,8>, 1024},
-  {1250, 125, 4, {10,5,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,1250,125,10,5,5,5>, (const void*)&axis_pass_static<float,false,1024,1250,125,10,5,5,5>, nullptr, nullptr, 1024},
-  {1500, 100, 3, {15,10,10}, 512, (const void*)&axis_pass_static<float,true,512,1500,100,15,10,10>, (const void*)&axis_pass_static<float,false,512,1500,100,15,10,10>, nullptr, nullptr, 512},
-  {1875, 125, 4, {15,5,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,1875,125,15,5,5,5>, (const void*)&axis_pass_static<float,false,1024,1875,125,15,5,5,5>, nullptr, nullptr, 1024},
-  {2160, 144, 3, {15,12,12}, 512, (const void*)&axis_pass_static<float,true,512,2160,144,15,12,12>, (const void*)&axis_pass_static<float,false,512,2160,144,15,12,12>, nullptr, nullptr, 512},
-  {2500, 250, 4, {10,10,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,2500,250,10,10,5,5>, (const void*)&axis_pass_static<float,false,1024,2500,250,10,10,5,5>, nullptr, nullptr, 1024},
-  {3000, 300, 4, {10,10,6,5}, 1024, (const void*)&axis_pass_static<float,true,1024,3000,300,10,10,6,5>, (const void*)&axis_pass_static<float,false,1024,3000,300,10,10,6,5>, nullptr, nullptr, 1024},
-  {3456, 288, 4, {12,6,6,8}, 1024, (const void*)&axis_pass_static<float,true,1024,3456,288,12,6,6,8>, (const void*)&axis_pass_static<float,false,1024,3456,288,12,6,6,8>, nullptr, nullptr, 1024},
-  {4000, 400, 4, {10,10,5,8}, 1024, (const void*)&axis_pass_static<float,true,1024,4000,400,10,10,5,8>, (const void*)&axis_pass_static<float,false,1024,4000,400,10,10,5,8>, nullptr, nullptr, 1024},
+  {3, 1, 1, {3}, 1024, (const void*)&axis_pass_static<float,true,1024,3,1,3>, (const void*)&axis_pass_static<float,false,1024,3,1,3>, nullptr, nullptr, 1024, 0},
+  {10, 1, 1, {10}, 1024, (const void*)&axis_pass_static<float,true,1024,10,1,10>, (const void*)&axis_pass_static<float,false,1024,10,1,10>, (const void*)&axis_pass_pipe<float,1024,false,16,10,1,10>, (const void*)&axis_pass_pipe<float,1024,true,0,10,1,10>, 1024, 16},
+  {24, 4, 2, {6,4}, 1024, (const void*)&axis_pass_static<float,true,1024,24,4,6,4>, (const void*)&axis_pass_static<float,false,1024,24,4,6,4>, (const void*)&axis_pass_pipe<float,1024,false,16,24,4,6,4>, (const void*)&axis_pass_pipe<float,1024,true,0,24,4,6,4>, 1024, 16},
+  {40, 5, 2, {5,8}, 1024, (const void*)&axis_pass_static<float,true,1024,40,5,5,8>, (const void*)&axis_pass_static<float,false,1024,40,5,5,8>, (const void*)&axis_pass_pipe<float,1024,false,16,40,5,5,8>, (const void*)&axis_pass_pipe<float,1024,true,0,40,5,5,8>, 1024, 16},
+  {64, 8, 2, {8,8}, 1024, (const void*)&axis_pass_static<float,true,1024,64,8,8,8>, (const void*)&axis_pass_static<float,false,1024,64,8,8,8>, (const void*)&axis_pass_pipe<float,1024,false,16,64,8,8,8>, (const void*)&axis_pass_pipe<float,1024,true,0,64,8,8,8>, 1024, 16},
+  {96, 8, 2, {12,8}, 1024, (const void*)&axis_pass_static<float,true,1024,96,8,12,8>, (const void*)&axis_pass_static<float,false,1024,96,8,12,8>, (const void*)&axis_pass_pipe<float,1024,false,16,96,8,12,8>, (const void*)&axis_pass_pipe<float,1024,true,0,96,8,12,8>, 1024, 16},
+  {135, 9, 3, {15,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,135,9,15,3,3>, (const void*)&axis_pass_static<float,false,1024,135,9,15,3,3>, (const void*)&axis_pass_pipe<float,1024,false,16,135,9,15,3,3>, (const void*)&axis_pass_pipe<float,1024,true,0,135,9,15,3,3>, 1024, 16},
+  {192, 12, 2, {12,16}, 512, (const void*)&axis_pass_static<float,true,512,192,12,12,16>, (const void*)&axis_pass_static<float,false,512,192,12,12,16>, (const void*)&axis_pass_pipe<float,512,false,16,192,12,12,16>, (const void*)&axis_pass_pipe<float,512,true,0,192,12,12,16>, 512, 16},
+  {250, 25, 3, {10,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,250,25,10,5,5>, (const void*)&axis_pass_static<float,false,1024,250,25,10,5,5>, (const void*)&axis_pass_pipe<float,1024,false,16,250,25,10,5,5>, (const void*)&axis_pass_pipe<float,1024,true,0,250,25,10,5,5>, 1024, 16},
+  {324, 54, 4, {6,6,3,3}, 1024, (const void*)&axis_pass_static<float,true,1024,324,54,6,6,3,3>, (const void*)&axis_pass_static<float,false,1024,324,54,6,6,3,3>, (const void*)&axis_pass_pipe<float,1024,false,16,324,54,6,6,3,3>, (const void*)&axis_pass_pipe<float,1024,true,0,324,54,6,6,3,3>, 1024, 16},
+  {432, 36, 3, {12,6,6}, 1024, (const void*)&axis_pass_static<float,true,1024,432,36,12,6,6>, (const void*)&axis_pass_static<float,false,1024,432,36,12,6,6>, (const void*)&axis_pass_pipe<float,1024,false,16,432,36,12,6,6>, (const void*)&axis_pass_pipe<float,1024,true,0,432,36,12,6,6>, 1024, 16},
+  {540, 36, 3, {15,6,6}, 512, (const void*)&axis_pass_static<float,true,512,540,36,15,6,6>, (const void*)&axis_pass_static<float,false,512,540,36,15,6,6>, (const void*)&axis_pass_pipe<float,512,false,8,540,36,15,6,6>, (const void*)&axis_pass_pipe<float,512,true,0,540,36,15,6,6>, 512, 8},
+  {675, 45, 3, {15,15,3}, 1024, (const void*)&axis_pass_static<float,true,1024,675,45,15,15,3>, (const void*)&axis_pass_static<float,false,1024,675,45,15,15,3>, (const void*)&axis_pass_pipe<float,1024,false,8,675,45,15,15,3>, (const void*)&axis_pass_pipe<float,1024,true,0,675,45,15,15,3>, 1024, 8},
+  {810, 54, 4, {15,6,3,3}, 512, (const void*)&axis_pass_static<float,true,512,810,54,15,6,3,3>, (const void*)&axis_pass_static<float,false,512,810,54,15,6,3,3>, (const void*)&axis_pass_pipe<float,512,false,8,810,54,15,6,3,3>, (const void*)&axis_pass_pipe<float,512,true,0,810,54,15,6,3,3>, 512, 8},
+  {1024, 64, 3, {16,8,8}, 1024, (const void*)&axis_pass_static<float,true,1024,1024,64,16,8,8>, (const void*)&axis_pass_static<float,false,1024,1024,64,16,8,8>, (const void*)&axis_pass_pipe<float,1024,false,8,1024,64,16,8,8>, (const void*)&axis_pass_pipe<float,1024,true,0,1024,64,16,8,8>, 1024, 8},
+  {1250, 125, 4, {10,5,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,1250,125,10,5,5,5>, (const void*)&axis_pass_static<float,false,1024,1250,125,10,5,5,5>, nullptr, nullptr, 1024, 0},
+  {1500, 100, 3, {15,10,10}, 512, (const void*)&axis_pass_static<float,true,512,1500,100,15,10,10>, (const void*)&axis_pass_static<float,false,512,1500,100,15,10,10>, nullptr, nullptr, 512, 0},
+  {1875, 125, 4, {15,5,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,1875,125,15,5,5,5>, (const void*)&axis_pass_static<float,false,1024,1875,125,15,5,5,5>, nullptr, nullptr, 1024, 0},
+  {2160, 144, 3, {15,12,12}, 512, (const void*)&axis_pass_static<float,true,512,2160,144,15,12,12>, (const void*)&axis_pass_static<float,false,512,2160,144,15,12,12>, nullptr, nullptr, 512, 0},
+  {2500, 250, 4, {10,10,5,5}, 1024, (const void*)&axis_pass_static<float,true,1024,2500,250,10,10,5,5>, (const void*)&axis_pass_static<float,false,1024,2500,250,10,10,5,5>, nullptr, nullptr, 1024, 0},
+  {3000, 300, 4, {10,10,6,5}, 1024, (const void*)&axis_pass_static<float,true,1024,3000,300,10,10,6,5>, (const void*)&axis_pass_static<float,false,1024,3000,300,10,10,6,5>, nullptr, nullptr, 1024, 0},
+  {3456, 288, 4, {12,6,6,8}, 1024, (const void*)&axis_pass_static<float,true,1024,3456,288,12,6,6,8>, (const void*)&axis_pass_static<float,false,1024,3456,288,12,6,6,8>, nullptr, nullptr, 1024, 0},
+  {4000, 400, 4, {10,10,5,8}, 1024, (const void*)&axis_pass_static<float,true,1024,4000,400,10,10,5,8>, (const void*)&axis_pass_static<float,false,1024,4000,400,10,10,5,8>, nullptr, nullptr, 1024, 0},
 };
 const int kPlansCount_f32_2 = 23;
 }  // namespace dfft

@@ -15,6 +15,7 @@ struct StaticPlan {
   const void* pipe_s; // axis_pass_pipe<T, LB, false, ...>: strided C2C, TMA-pipelined (or null)
   const void* pipe_c; // axis_pass_pipe<T, LB, true, ...>: contiguous C2C, bulk-copy pipelined
   int pipe_lb;        // __launch_bounds__ of the pipelined kernels
+  int pipe_cs;        // columns per tile compiled into the strided pipelined kernel
 };
 
 struct StaticPlanTable {

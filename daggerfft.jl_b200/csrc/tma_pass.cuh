@@ -22,7 +22,11 @@
 // shared-memory FFT.  Ordering: threads write the tile, fence.proxy.async,
 // barrier, then one thread issues the store; a buffer is reloaded only after
 // cp.async.bulk.wait_group.read confirms its previous store has read it.
-// Stage twiddles are copied once per CTA into shared memory (StageTw layout).
+// The contiguous variant copies the stage twiddles once per CTA into shared
+// memory (StageTw layout); the strided variant reads the L-entry table
+// through L1 (in its cfast mapping a warp needs only two twiddles per
+// element), which keeps its shared-memory footprint (three 64 KB tiles for
+// L = 512) small enough that L1 keeps its share of the SRAM.
 //
 // Every mbarrier wait is bounded (~2 s); on expiry the kernel records
 // DFFT_DEVERR_TMA_TIMEOUT in the device error word, waits (bounded) for the
@@ -168,7 +172,9 @@ __device__ __forceinline__ void pipe_issue_store(const PassDesc& d, const CUtens
 // region, the buffer stride and (host-checked) every box offset inside a
 // buffer are multiples of 128 bytes; the kernel re-checks and reports
 // DFFT_DEVERR_TMA_ALIGN instead of issuing a misaligned copy.
-template <typename T, int LB, bool CONTIG, int L, int P, int... Rs>
+// CS: columns per tile fixed at compile time (strided variant; 0 = runtime,
+// contiguous variant).
+template <typename T, int LB, bool CONTIG, int CS, int L, int P, int... Rs>
 __global__ void __launch_bounds__(LB) axis_pass_pipe(const PassDesc d,
                                                      const __grid_constant__ CUtensorMap tin,
                                                      const __grid_constant__ CUtensorMap tout,
@@ -185,6 +191,7 @@ __global__ void __launch_bounds__(LB) axis_pass_pipe(const PassDesc d,
   const int tid = threadIdx.x;
   int c, t;
   if (CONTIG) { t = tid % P; c = tid / P; }
+  else if (CS > 0) { c = tid % CS; t = tid / CS; }
   else { c = tid % g.C; t = tid / g.C; }
   if (tid == 0) {
     for (int b = 0; b < kTmaBufs; ++b) mbar_init(&bars[b], 1);
@@ -205,6 +212,7 @@ __global__ void __launch_bounds__(LB) axis_pass_pipe(const PassDesc d,
   if (s_abort) return;  // misaligned layout: nothing was issued
   const int C = g.C;
   const StageTw<V> tw{stw};
+  const GlobalTw<V> twl{reinterpret_cast<const V*>(d.tw2)};
   const long long first = blockIdx.x;
   const long long step = gridDim.x;
   int issued[kTmaBufs] = {0, 0, 0};  // loads issued per buffer (thread 0)
@@ -231,9 +239,15 @@ __global__ void __launch_bounds__(LB) axis_pass_pipe(const PassDesc d,
       static_stages<T, L, P, true, true, 1, 1, 0, StrideCol<V>, PadCol<V>, StrideCol<V>, StageTw<V>,
                     Rs...>(d, t, dense, pad, dense, tw, 0, 0, true);
     } else {
-      const StrideCol<V> col{sb + c, C};
-      static_stages<T, L, P, true, true, 1, 1, 0, StrideCol<V>, StrideCol<V>, StrideCol<V>,
-                    StageTw<V>, Rs...>(d, t, col, col, col, tw, 0, 0, true);
+      if constexpr (CS > 0) {
+        const StrideColC<V, CS> col{sb + c};
+        static_stages<T, L, P, true, true, 1, 1, 0, StrideColC<V, CS>, StrideColC<V, CS>,
+                      StrideColC<V, CS>, GlobalTw<V>, Rs...>(d, t, col, col, col, twl, 0, 0, true);
+      } else {
+        const StrideCol<V> col{sb + c, C};
+        static_stages<T, L, P, true, true, 1, 1, 0, StrideCol<V>, StrideCol<V>, StrideCol<V>,
+                      GlobalTw<V>, Rs...>(d, t, col, col, col, twl, 0, 0, true);
+      }
     }
     fence_proxy_async_smem();
     __syncthreads();

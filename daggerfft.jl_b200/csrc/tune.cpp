@@ -11,6 +11,7 @@
 // a text file.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <fstream>
 #include <map>
 #include <mutex>
@@ -115,6 +116,9 @@ Pass tune_pass(const PassSpec& s) {
   cudaEventCreate(&e1);
   float best = 1e30f;
   int bv = VARIANT_AUTO, bc = 0;
+  // DFFT_TUNE_VERBOSE=1 prints every candidate's time to stderr
+  const char* ev = std::getenv("DFFT_TUNE_VERBOSE");
+  const bool verbose = ev && ev[0] && ev[0] != '0';
   for (auto& vc : cands) {
     PassSpec t = s;
     t.variant = vc.first;
@@ -137,6 +141,9 @@ Pass tune_pass(const PassSpec& s) {
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     ms /= reps;
+    if (verbose)
+      std::fprintf(stderr, "dfft tune: L=%d I=%lld O=%lld variant=%d C=%d threads=%u grid=%u smem=%zu %.4f ms\n",
+                   s.L, s.I, s.O, vc.first, vc.second, p.block.x, p.grid.x, p.smem, ms);
     if (ms < best) { best = ms; bv = vc.first; bc = vc.second; }
   }
   cleanup();

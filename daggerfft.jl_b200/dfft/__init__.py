@@ -13,4 +13,8 @@ from .api import (DHT, FFT, FFT_, GPU_PLAN_CACHE, HC2R, IFFT, IFFT_, IRFFT, IRFF
                   apply_gpu_fft_, empty_like_layout, fft, fft_, get_or_create_gpu_plan,
                   gpu_cleanup_plans, gpu_plan_transform, ifft, ifft_, irfft, rfft)
 
+from .darray import (Blocks, CudaCopier, DArray, Workspace, collect, compute_overlap,
+                     create_gpu_workspace, distribute, empty_darray, gpu_cleanup_workspace_,
+                     gpu_coalesced_redistribute_, gpu_fft_, gpu_ifft_)
+
 __version__ = "0.1.0"

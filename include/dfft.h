@@ -153,6 +153,38 @@ DFFT_API int dfft_wisdom_import(const char* path);
 DFFT_API int dfft_wisdom_forget(void);
 DFFT_API int dfft_wisdom_size(int* n);
 
+/* ---- redistribution between blockings --------------------------------
+ *
+ * One sub-block copy: `count` elements per dim from chunk `src` (column-major
+ * extents src_dims) starting at src_start (0-based) to chunk `dst` at
+ * dst_start.  A flat pack/unpack buffer is a chunk whose extents equal
+ * `count` (x fastest, as pack_data!/unpack_data! lay it out,
+ * src/fft.jl:180-214).  Replaces the per-pattern launches of
+ * local_copy_kernel!, pack_kernel! and unpack_kernel!
+ * (src/fftgpu.jl:367-385, 417-495).
+ */
+typedef struct {
+  const void* src;
+  void* dst;
+  int64_t src_start[3];
+  int64_t dst_start[3];
+  int64_t src_dims[3];
+  int64_t dst_dims[3];
+  int64_t count[3];
+} dfft_block_copy;
+
+typedef struct dfft_copy_plan_s* dfft_copy_plan;
+
+/* A device-resident list of block copies executed by one launch (the
+ * pattern list of create_gpu_workspace, src/fftgpu.jl:126-318). */
+DFFT_API int dfft_copy_plan_create(dfft_copy_plan* plan, const dfft_block_copy* blocks, int nblocks,
+                                   int elem_bytes);
+/* Runs every copy of the plan (the LOCAL_COPIES / PACK_SEND / RECV_UNPACK
+ * phases of gpu_flat_redistribute!, src/fftgpu.jl:324-415). */
+DFFT_API int dfft_copy_plan_execute(dfft_copy_plan plan, void* stream);
+DFFT_API int dfft_copy_plan_bytes(dfft_copy_plan plan, int64_t* bytes);
+DFFT_API int dfft_copy_plan_destroy(dfft_copy_plan plan);
+
 /* Thread-local description of the last error. */
 DFFT_API const char* dfft_last_error(void);
 DFFT_API const char* dfft_status_string(int status);
