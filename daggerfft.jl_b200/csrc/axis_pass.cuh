@@ -125,7 +125,14 @@ __device__ __forceinline__ typename cvec<T>::type load_elem(const IoAny& io, lon
       V A = p[b + k * io.sk];
       V B = cconj(p[b + (io.n - k) * io.sk]);
       if (k == 0) { A.y = (T)0; B.y = (T)0; }  // c2r ignores Im X_0 and Im X_{n}
-      V wk = cconj(ldg_c(reinterpret_cast<const V*>(io.w) + k));
+      V wk;
+      if (io.w) {
+        wk = cconj(ldg_c(reinterpret_cast<const V*>(io.w) + k));
+      } else {  // exp(+2 pi i k / (2n)), computed in the kernel
+        double sn, cs;
+        sincospi((double)k / (double)io.n, &sn, &cs);
+        wk = mk<V>((T)cs, (T)sn);
+      }
       return cadd(cadd(A, B), cmul_pi(cmul(wk, csub(A, B))));
     }
     case IO_HERM_FULL: {
@@ -284,6 +291,19 @@ template <typename V> struct StageTw {
     return p[off + jm * (R - 1) + r - 1];
   }
 };
+// Twiddles computed in the kernel (no table in memory): exp(-2 pi i jm r ts / L)
+// with the CUDA math library's sincospi in double precision.
+template <typename V> struct ComputedTw {
+  int L;
+  __device__ __forceinline__ V w(int off, int jm, int r, int R, int ts) const {
+    typedef typename scalar_of<V>::type S;
+    const long long m = ((long long)jm * r * ts) % L;
+    double sn, cs;
+    sincospi(2.0 * (double)m / (double)L, &sn, &cs);
+    return mk<V>((S)cs, (S)-sn);
+  }
+};
+
 // The same stage-major table read from global memory through L1.
 template <typename V> struct StageTwG {
   const V* p;
@@ -453,18 +473,25 @@ __global__ void __launch_bounds__(LB) axis_pass_static(const PassDesc d) {
 // Dynamic-plan kernel (fallback for lengths without a static plan).
 // ---------------------------------------------------------------------------
 
-template <typename T, int R, int EMAX>
+template <typename T, int R, int EMAX, bool CTW>
 __device__ __noinline__ void dyn_stage(const PassDesc& d, int s, int t, typename cvec<T>::type* col,
                                        const typename cvec<T>::type* tw, long long ib, long long ob,
                                        bool cv) {
   typedef typename cvec<T>::type V;
   const PadCol<V> c{col};
-  const GlobalTw<V> g{tw};
-  stage_body<T, R, EMAX / R, false, false>(d, d.L, d.P, d.ns[s], d.tws[s], 0, s == 0,
-                                           s == d.nst - 1, t, c, c, g, ib, ob, cv);
+  if constexpr (CTW) {
+    const ComputedTw<V> g{d.L};
+    stage_body<T, R, EMAX / R, false, false>(d, d.L, d.P, d.ns[s], d.tws[s], 0, s == 0,
+                                             s == d.nst - 1, t, c, c, g, ib, ob, cv);
+  } else {
+    const GlobalTw<V> g{tw};
+    stage_body<T, R, EMAX / R, false, false>(d, d.L, d.P, d.ns[s], d.tws[s], 0, s == 0,
+                                             s == d.nst - 1, t, c, c, g, ib, ob, cv);
+  }
 }
 
-template <typename T, int EMAX>
+// CTW: twiddles computed in the kernel instead of read from d.tw (no table).
+template <typename T, int EMAX, bool CTW = false>
 __global__ void __launch_bounds__(1024) axis_pass_dynamic(const PassDesc d) {
   typedef typename cvec<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -474,16 +501,16 @@ __global__ void __launch_bounds__(1024) axis_pass_dynamic(const PassDesc d) {
   const V* tw = reinterpret_cast<const V*>(d.tw);
   for (int s = 0; s < d.nst; ++s) {
     switch (d.radix[s]) {
-      case 1: dyn_stage<T, 1, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
-      case 2: dyn_stage<T, 2, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
-      case 3: dyn_stage<T, 3, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
-      case 4: dyn_stage<T, 4, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
-      case 5: dyn_stage<T, 5, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
-      case 7: dyn_stage<T, 7, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
-      case 8: dyn_stage<T, 8, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
-      case 11: dyn_stage<T, 11, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
-      case 13: dyn_stage<T, 13, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
-      case 16: dyn_stage<T, 16, EMAX>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 1: dyn_stage<T, 1, EMAX, CTW>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 2: dyn_stage<T, 2, EMAX, CTW>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 3: dyn_stage<T, 3, EMAX, CTW>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 4: dyn_stage<T, 4, EMAX, CTW>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 5: dyn_stage<T, 5, EMAX, CTW>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 7: dyn_stage<T, 7, EMAX, CTW>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 8: dyn_stage<T, 8, EMAX, CTW>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 11: dyn_stage<T, 11, EMAX, CTW>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 13: dyn_stage<T, 13, EMAX, CTW>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
+      case 16: dyn_stage<T, 16, EMAX, CTW>(d, s, x.t, col, tw, x.ib, x.ob, x.cv); break;
       default: break;
     }
   }

@@ -190,8 +190,8 @@ __global__ void __launch_bounds__(LB) axis_pass_pipe(const PassDesc d,
   V* work = bufs + kTmaBufs * buf_elems;
   const int tid = threadIdx.x;
   int c, t;
-  if (CONTIG) { t = tid % P; c = tid / P; }
-  else if (CS > 0) { c = tid % CS; t = tid / CS; }
+  if constexpr (CONTIG) { t = tid % P; c = tid / P; }
+  else if constexpr (CS > 0) { c = tid % CS; t = tid / CS; }
   else { c = tid % g.C; t = tid / g.C; }
   if (tid == 0) {
     for (int b = 0; b < kTmaBufs; ++b) mbar_init(&bars[b], 1);

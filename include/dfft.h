@@ -185,6 +185,22 @@ DFFT_API int dfft_copy_plan_execute(dfft_copy_plan plan, void* stream);
 DFFT_API int dfft_copy_plan_bytes(dfft_copy_plan plan, int64_t* bytes);
 DFFT_API int dfft_copy_plan_destroy(dfft_copy_plan plan);
 
+/*
+ * irfft of a ComplexF32 half-spectrum over all dims (dims = 1..ndim, real
+ * length shape[0] along dim 1) that allocates no device memory.  No
+ * counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc when they transform (code inside another framework's memory
+ * pool, or held to a fixed HBM budget).  The intermediate lives in a static
+ * device array of 2^21 ComplexF32 (16 MiB) that every GPU loading the
+ * library keeps until exit; larger sizes return DFFT_ERROR_INVALID_VALUE.
+ * Calls that overlap on the GPU race on that array.  The first call on a
+ * device looks up the array's address; make it before any stream capture.
+ * in: (shape[0]/2+1, shape[1], shape[2]) ComplexF32, out: shape Float32,
+ * both column-major device memory.
+ */
+DFFT_API int dfft_irfft_noalloc_f32(const void* in, void* out, int ndim, const int64_t* shape,
+                                    void* stream);
+
 /* Thread-local description of the last error. */
 DFFT_API const char* dfft_last_error(void);
 DFFT_API const char* dfft_status_string(int status);
