@@ -59,6 +59,12 @@ struct IoAny {
   int r2r;           // FFTW kind for IO_R2R
   int n;             // logical extent (see the kinds)
   const void* w;     // twiddle table for the kinds that need one
+  // Bluestein wrapping (chirp-z) of any kind: element k < chirp_n is
+  // multiplied by chirp[k] after loading / before storing, elements
+  // k >= chirp_n load as zero and are not stored; mul[k] multiplies a load.
+  const void* chirp;
+  const void* mul;
+  int chirp_n;
 };
 
 struct PassDesc {
@@ -105,7 +111,7 @@ template <typename V> __device__ __forceinline__ V ldg_c(const V* p) { return __
 // ---------------------------------------------------------------------------
 
 template <typename T>
-__device__ __forceinline__ typename cvec<T>::type load_elem(const IoAny& io, long long b, int k) {
+__device__ __forceinline__ typename cvec<T>::type load_raw(const IoAny& io, long long b, int k) {
   typedef typename cvec<T>::type V;
   const T z = (T)0;
   switch (io.kind) {
@@ -185,8 +191,8 @@ __device__ __forceinline__ typename cvec<T>::type load_elem(const IoAny& io, lon
 }
 
 template <typename T>
-__device__ __forceinline__ void store_elem(const IoAny& io, long long b, int k,
-                                           typename cvec<T>::type v, T s) {
+__device__ __forceinline__ void store_raw(const IoAny& io, long long b, int k,
+                                          typename cvec<T>::type v, T s) {
   typedef typename cvec<T>::type V;
   switch (io.kind) {
     case IO_CPLX:
@@ -246,6 +252,30 @@ __device__ __forceinline__ void store_elem(const IoAny& io, long long b, int k,
       }
     }
   }
+}
+
+// Element access with the optional Bluestein chirp / filter multiply.
+template <typename T>
+__device__ __forceinline__ typename cvec<T>::type load_elem(const IoAny& io, long long b, int k) {
+  typedef typename cvec<T>::type V;
+  if (io.chirp) {
+    if (k >= io.chirp_n) return mk<V>((T)0, (T)0);
+    return cmul(load_raw<T>(io, b, k), ldg_c(reinterpret_cast<const V*>(io.chirp) + k));
+  }
+  V v = load_raw<T>(io, b, k);
+  if (io.mul) v = cmul(v, ldg_c(reinterpret_cast<const V*>(io.mul) + k));
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ void store_elem(const IoAny& io, long long b, int k,
+                                           typename cvec<T>::type v, T s) {
+  typedef typename cvec<T>::type V;
+  if (io.chirp) {
+    if (k >= io.chirp_n) return;
+    v = cmul(v, ldg_c(reinterpret_cast<const V*>(io.chirp) + k));
+  }
+  store_raw<T>(io, b, k, v, s);
 }
 
 // ---------------------------------------------------------------------------

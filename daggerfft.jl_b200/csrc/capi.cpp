@@ -56,7 +56,7 @@ int dfft_plan_workspace_bytes(dfft_plan plan, size_t* bytes) {
   return guarded([&] {
     dfft::Plan* p = impl(plan);
     if (!bytes) throw Error{DFFT_ERROR_INVALID_VALUE, "bytes is NULL"};
-    *bytes = p->work_bytes;
+    *bytes = p->work_bytes + p->chirp_bytes;
   });
 }
 

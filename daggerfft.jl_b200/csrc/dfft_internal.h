@@ -35,7 +35,7 @@ std::shared_ptr<DevTable> twiddle_table(int dbl, long long D, long long a, long 
                                         bool conj);
 
 // One kernel launch of a plan.
-enum BufId : int { BUF_IN = 0, BUF_OUT = 1, BUF_WORK = 2 };
+enum BufId : int { BUF_IN = 0, BUF_OUT = 1, BUF_WORK = 2, BUF_CHIRP = 3 };
 
 struct Pass {
   PassDesc d{};
@@ -70,7 +70,13 @@ struct PassSpec {
   bool fast_io = false;      // plain complex in/out
   int variant = VARIANT_AUTO;
   int C = 0;                 // columns per CTA (0: heuristic)
+  std::vector<std::shared_ptr<DevTable>> keep;  // tables the IoAny sides point into
 };
+
+// Appends the passes of one axis: a single pass, or the two passes of
+// Bluestein's algorithm (via a scratch of Q*M complex elements) when no
+// single-pass kernel handles the length.  Returns the scratch bytes needed.
+size_t add_axis_passes(std::vector<Pass>& out, const PassSpec& s, unsigned flags, int src, int dst);
 
 // Builds a launchable pass; throws Error on unsupported sizes.
 Pass make_pass(const PassSpec& s);

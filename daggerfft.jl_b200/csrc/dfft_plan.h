@@ -20,6 +20,8 @@ struct Plan {
   std::vector<Pass> passes;
   void* work = nullptr;           // plan-owned workspace (C2R over several dims)
   size_t work_bytes = 0;
+  void* chirp = nullptr;          // Bluestein scratch (Q*M complex per axis, max over axes)
+  size_t chirp_bytes = 0;
   ~Plan();
   size_t in_bytes() const;
   size_t out_bytes() const;

@@ -354,6 +354,7 @@ Pass make_pass(const PassSpec& s) {
   d.scale = s.scale;
   d.in = s.in;
   d.out = s.out;
+  for (auto& t : s.keep) p.tables.push_back(t);
   const size_t col_bytes = (size_t)ld * esz;
 
   if (variant == VARIANT_PIPE) {
@@ -494,6 +495,184 @@ cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream)
   }
   void* args[] = {&d};
   return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
+}
+
+}  // namespace dfft
+
+namespace dfft {
+
+// ---------------------------------------------------------------------------
+// Bluestein (chirp-z) for lengths no single-pass kernel handles.
+//   X_k = w_k sum_n (x_n w_n) b_{k-n},  w_n = exp(s i pi n^2 / L),
+//   b_m = conj(w_m), s = -1 (forward) or +1 (inverse);
+// the convolution runs as FFT_M, a pointwise multiply by
+// Bhat = FFT_M(B) / M (B the wrapped b), and an inverse FFT_M, with M the
+// smallest 5-smooth length >= 2L-1.
+// ---------------------------------------------------------------------------
+
+static int smooth5_at_least(int n) {
+  for (int m = n;; ++m) {
+    int r = m;
+    for (int p : {2, 3, 5})
+      while (r % p == 0) r /= p;
+    if (r == 1) return m;
+  }
+}
+
+static std::shared_ptr<DevTable> upload(int dbl, const std::vector<long double>& re,
+                                        const std::vector<long double>& im) {
+  const size_t n = re.size(), esz = dbl ? 16 : 8;
+  std::vector<unsigned char> host(esz * (n ? n : 1));
+  for (size_t k = 0; k < n; ++k) {
+    if (dbl) { double v[2] = {(double)re[k], (double)im[k]}; std::memcpy(&host[esz * k], v, esz); }
+    else { float v[2] = {(float)re[k], (float)im[k]}; std::memcpy(&host[esz * k], v, esz); }
+  }
+  auto t = std::make_shared<DevTable>();
+  cuda_check(cudaGetDevice(&t->device), "cudaGetDevice");
+  t->bytes = host.size();
+  cuda_check(cudaMalloc(&t->p, t->bytes), "cudaMalloc(bluestein)");
+  cuda_check(cudaMemcpy(t->p, host.data(), t->bytes, cudaMemcpyHostToDevice), "cudaMemcpy(bluestein)");
+  return t;
+}
+
+struct BluesteinTables {
+  int M;
+  std::shared_ptr<DevTable> chirp, bhat;
+};
+
+static BluesteinTables bluestein_tables(int dbl, int L, int sgn) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, int>, std::pair<int, std::pair<std::weak_ptr<DevTable>,
+                                                                           std::weak_ptr<DevTable>>>> cache;
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  auto key = std::make_tuple(dev, dbl, L, sgn);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) {
+    auto a = it->second.second.first.lock();
+    auto b = it->second.second.second.lock();
+    if (a && b) return BluesteinTables{it->second.first, a, b};
+  }
+  const int M = smooth5_at_least(2 * L - 1);
+  const long double pi = acosl(-1.0L);
+  // chirp w_n = exp(s i pi n^2 / L), n^2 reduced exactly modulo 2L
+  std::vector<long double> wr(L), wi(L);
+  for (int n = 0; n < L; ++n) {
+    const long long m = ((long long)n * n) % (2LL * L);
+    const long double a = pi * (long double)m / (long double)L;
+    wr[n] = cosl(a);
+    wi[n] = sgn * sinl(a);
+  }
+  // B (wrapped conj chirp), transformed in double precision on the device
+  std::vector<double> B(2 * (size_t)M, 0.0);
+  for (int m = 0; m < L; ++m) {
+    B[2 * m] = (double)wr[m];
+    B[2 * m + 1] = (double)-wi[m];
+    if (m > 0) {
+      B[2 * (M - m)] = (double)wr[m];
+      B[2 * (M - m) + 1] = (double)-wi[m];
+    }
+  }
+  void* dB = nullptr;
+  cuda_check(cudaMalloc(&dB, B.size() * sizeof(double)), "cudaMalloc(bluestein B)");
+  std::vector<double> F(B.size());
+  try {
+    cuda_check(cudaMemcpy(dB, B.data(), B.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy");
+    PassSpec ps;
+    ps.dbl = 1;
+    ps.L = M;
+    ps.I = 1;
+    ps.O = 1;
+    ps.in.kind = ps.out.kind = IO_CPLX;
+    ps.in.si = ps.out.si = 1;
+    ps.in.so = ps.out.so = M;
+    ps.in.sk = ps.out.sk = 1;
+    ps.fast_io = true;
+    ps.variant = VARIANT_DIRECT;
+    Pass fp;
+    try {
+      fp = make_pass(ps);
+    } catch (const Error&) {
+      ps.variant = VARIANT_DYNAMIC;
+      fp = make_pass(ps);
+    }
+    cuda_check(launch_pass(fp, dB, dB, 0), "bluestein filter FFT");
+    cuda_check(cudaMemcpy(F.data(), dB, F.size() * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+  } catch (...) {
+    cudaFree(dB);
+    throw;
+  }
+  cudaFree(dB);
+  std::vector<long double> br(M), bi(M);
+  for (int k = 0; k < M; ++k) {
+    br[k] = (long double)F[2 * k] / M;
+    bi[k] = (long double)F[2 * k + 1] / M;
+  }
+  BluesteinTables t{M, upload(dbl, wr, wi), upload(dbl, br, bi)};
+  cache[key] = {M, {t.chirp, t.bhat}};
+  return t;
+}
+
+size_t add_axis_passes(std::vector<Pass>& out, const PassSpec& s, unsigned flags, int src, int dst) {
+  try {
+    Pass p = plan_pass(s, flags);
+    p.src = src;
+    p.dst = dst;
+    out.push_back(std::move(p));
+    return 0;
+  } catch (const Error& e) {
+    if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
+  }
+  const int L = s.L;
+  if (L > (1 << 20)) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "length too large for Bluestein"};
+  // the outer direction is in the tables; the inner FFT_M pair is forward
+  // then inverse
+  BluesteinTables bt = bluestein_tables(s.dbl, L, s.inverse ? +1 : -1);
+  const int M = bt.M;
+  const size_t csz = s.dbl ? 16 : 8;
+  PassSpec a = s;
+  a.L = M;
+  a.inverse = 0;
+  a.scale = 1.0;
+  a.fast_io = false;
+  a.epi = false;
+  a.variant = VARIANT_AUTO;
+  a.C = 0;
+  a.in.chirp = bt.chirp->p;
+  a.in.chirp_n = L;
+  a.out = IoAny{};
+  a.out.kind = IO_CPLX;
+  a.out.si = 1;
+  a.out.so = s.I * M;
+  a.out.sk = s.I;
+  a.keep.push_back(bt.chirp);
+  PassSpec b = s;
+  b.L = M;
+  b.inverse = 1;
+  b.fast_io = false;
+  b.epi = false;
+  b.variant = VARIANT_AUTO;
+  b.C = 0;
+  b.in = IoAny{};
+  b.in.kind = IO_CPLX;
+  b.in.si = 1;
+  b.in.so = s.I * M;
+  b.in.sk = s.I;
+  b.in.mul = bt.bhat->p;
+  b.out.chirp = bt.chirp->p;
+  b.out.chirp_n = L;
+  b.keep.push_back(bt.chirp);
+  b.keep.push_back(bt.bhat);
+  Pass pa = make_pass(a);
+  pa.src = src;
+  pa.dst = BUF_CHIRP;
+  Pass pb = make_pass(b);
+  pb.src = BUF_CHIRP;
+  pb.dst = dst;
+  out.push_back(std::move(pa));
+  out.push_back(std::move(pb));
+  return (size_t)(s.I * s.O) * (size_t)M * csz;
 }
 
 }  // namespace dfft

@@ -82,6 +82,33 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
   if (method == DFFT_MIXED && !(is_c2c(transform) && !dbl))
     throw Error{DFFT_ERROR_INVALID_VALUE, "the mixed form supports ComplexF32 FFT/IFFT only"};
 
+  size_t chirp_bytes = 0;
+  auto add = [&](const PassSpec& sp, int src, int dst) {
+    size_t w = add_axis_passes(P->passes, sp, flags, src, dst);
+    if (w > chirp_bytes) chirp_bytes = w;
+  };
+  // does a single pass handle FFT length L?  (otherwise Bluestein, and the
+  // real transforms take their full-length form)
+  auto single_ok = [&](int L, long long I, long long O) {
+    PassSpec t;
+    t.dbl = dbl;
+    t.L = L;
+    t.I = I;
+    t.O = O;
+    t.in.kind = t.out.kind = IO_CPLX;
+    t.in.si = t.out.si = 1;
+    t.in.so = t.out.so = I * L;
+    t.in.sk = t.out.sk = I;
+    t.variant = VARIANT_AUTO;
+    try {
+      make_pass(t);
+      return true;
+    } catch (const Error& e) {
+      if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
+      return false;
+    }
+  };
+
   if (is_c2c(transform)) {
     const bool inv = is_inverse_c2c(transform);
     P->in_elem = P->out_elem = csz;
@@ -98,11 +125,8 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
       s.in = io(IO_CPLX, s.I, S[a]);
       s.out = io(IO_CPLX, s.I, S[a]);
       s.fast_io = true;
-      Pass p = plan_pass(s, flags);
-      p.src = src;
-      p.dst = BUF_OUT;
+      add(s, src, BUF_OUT);
       src = BUF_OUT;
-      P->passes.push_back(std::move(p));
     }
   } else if (is_rfft(transform)) {
     if (ax.empty()) throw Error{DFFT_ERROR_INVALID_VALUE, "rfft needs at least one dim"};
@@ -116,21 +140,20 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
     PassSpec s;
     s.dbl = dbl;
     split(S, a0, &s.I, &s.O);
-    if (n % 2 == 0) {
+    if (n % 2 == 0 && single_ok((int)(n / 2), s.I, s.O)) {
       s.L = (int)(n / 2);
       s.in = io(IO_REAL_PAIR, s.I, n);
       s.out = io(IO_CPLX, s.I, H[a0]);
       s.epi = true;
     } else {
+      // odd length (or a half length no single pass handles): the real
+      // input as complex, full-length FFT, first n/2+1 outputs kept
       s.L = (int)n;
       s.in = io(IO_REAL, s.I, n);
       s.out = io(IO_TRUNC, s.I, H[a0]);
       s.out.n = (int)(n / 2);
     }
-    Pass p0 = plan_pass(s, flags);
-    p0.src = BUF_IN;
-    p0.dst = BUF_OUT;
-    P->passes.push_back(std::move(p0));
+    add(s, BUF_IN, BUF_OUT);
     for (size_t i = 1; i < ax.size(); ++i) {
       const int a = ax[i];
       PassSpec c;
@@ -140,10 +163,7 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
       c.in = io(IO_CPLX, c.I, H[a]);
       c.out = io(IO_CPLX, c.I, H[a]);
       c.fast_io = true;
-      Pass p = plan_pass(c, flags);
-      p.src = BUF_OUT;
-      p.dst = BUF_OUT;
-      P->passes.push_back(std::move(p));
+      add(c, BUF_OUT, BUF_OUT);
     }
   } else if (is_irfft(transform)) {
     if (ax.empty()) throw Error{DFFT_ERROR_INVALID_VALUE, "irfft needs at least one dim"};
@@ -172,24 +192,22 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
       c.in = io(IO_CPLX, c.I, S[a]);
       c.out = io(IO_CPLX, c.I, S[a]);
       c.fast_io = true;
-      Pass p = plan_pass(c, flags);
-      p.src = src;
-      p.dst = work;
+      add(c, src, work);
       src = work;
-      P->passes.push_back(std::move(p));
     }
-    if (src == BUF_WORK || (!destroy && ax.size() > 1)) {
-      P->work_bytes = (size_t)(S[0] * S[1] * S[2]) * csz;
-    }
+    if (src == BUF_WORK) P->work_bytes = (size_t)(S[0] * S[1] * S[2]) * csz;
     PassSpec s;
     s.dbl = dbl;
     split(S, a0, &s.I, &s.O);
     s.inverse = 1;
     s.scale = 1.0 / (double)d;
-    if (d % 2 == 0) {
+    if (d % 2 == 0 && single_ok((int)(d / 2), s.I, s.O)) {
       s.L = (int)(d / 2);
       s.in = io(IO_HERM_PAIR, s.I, S[a0]);
       s.in.n = s.L;
+      auto w = twiddle_table(dbl, d, 1, 0, (int)(d / 2) + 1, false);
+      s.in.w = w->p;
+      s.keep.push_back(w);
       s.out = io(IO_REAL_PAIR, s.I, d);
     } else {
       s.L = (int)d;
@@ -197,15 +215,7 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
       s.in.n = (int)d;
       s.out = io(IO_REAL, s.I, d);
     }
-    Pass p = plan_pass(s, flags);
-    if (d % 2 == 0) {
-      auto w = twiddle_table(dbl, d, 1, 0, (int)(d / 2) + 1, false);
-      p.tables.push_back(w);
-      p.d.in.w = w->p;
-    }
-    p.src = src;
-    p.dst = BUF_OUT;
-    P->passes.push_back(std::move(p));
+    add(s, src, BUF_OUT);
   } else {  // DFFT_R2R
     if (!r2r_kinds && !ax.empty()) throw Error{DFFT_ERROR_INVALID_VALUE, "r2r_kinds is NULL"};
     P->in_elem = P->out_elem = rsz;
@@ -253,15 +263,14 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
         default:
           throw Error{DFFT_ERROR_UNKNOWN_TRANSFORM, "Unknown transform type"};
       }
-      Pass p = plan_pass(s, flags);
-      if (win) { p.tables.push_back(win); p.d.in.w = win->p; }
-      if (wout) { p.tables.push_back(wout); p.d.out.w = wout->p; }
-      p.src = src;
-      p.dst = BUF_OUT;
+      if (win) { s.in.w = win->p; s.keep.push_back(win); }
+      if (wout) { s.out.w = wout->p; s.keep.push_back(wout); }
+      add(s, src, BUF_OUT);
       src = BUF_OUT;
-      P->passes.push_back(std::move(p));
     }
   }
+  P->chirp_bytes = chirp_bytes;
+  if (chirp_bytes) cuda_check(cudaMalloc(&P->chirp, chirp_bytes), "cudaMalloc(bluestein scratch)");
   if (P->work_bytes) {
     cuda_check(cudaMalloc(&P->work, P->work_bytes), "cudaMalloc(workspace)");
   }
@@ -269,11 +278,12 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
 }
 
 Plan::~Plan() {
-  if (work) {
+  if (work || chirp) {
     int cur = -1;
     cudaGetDevice(&cur);
     if (cur != device) cudaSetDevice(device);
-    cudaFree(work);
+    if (work) cudaFree(work);
+    if (chirp) cudaFree(chirp);
     if (cur != device && cur >= 0) cudaSetDevice(cur);
   }
 }
@@ -292,7 +302,7 @@ void execute_plan(const Plan* P, const void* in, void* out, cudaStream_t stream)
   }
   for (const Pass& p : P->passes) {
     if (err != cudaSuccess) break;
-    void* bufs[3] = {const_cast<void*>(in), out, P->work};
+    void* bufs[4] = {const_cast<void*>(in), out, P->work, P->chirp};
     err = launch_pass(p, bufs[p.src], bufs[p.dst], stream);
   }
   if (cur != P->device) cudaSetDevice(cur);

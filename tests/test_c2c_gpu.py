@@ -11,11 +11,13 @@ from helpers import rand, rel, to_gpu, to_np, tol_for
 
 pytestmark = pytest.mark.gpu
 
-# every 5-smooth length up to 64, the configuration edges, large powers of two,
-# odd primes, and lengths that only the dynamic kernel covers (7/11/13 factors)
+# every length up to 64 (primes above 13 go through Bluestein), the
+# configuration edges, large powers of two, lengths only the dynamic kernel
+# covers (7/11/13 factors), and large primes
 LENGTHS_1D = sorted(set(list(range(1, 65)) + [
     80, 96, 100, 120, 125, 128, 160, 192, 243, 256, 384, 500, 512, 625, 729, 1000, 1024,
-    1536, 2048, 3072, 4096, 8192, 77, 91, 98, 143, 169, 343, 1001, 2002, 4914]))
+    1536, 2048, 3072, 4096, 8192, 77, 91, 98, 143, 169, 343, 1001, 2002, 4914,
+    127, 251, 509, 1009, 2039, 4093]))
 
 
 @pytest.mark.parametrize("n", LENGTHS_1D)
@@ -40,7 +42,7 @@ def test_1d_inverse(n, dtype):
 
 
 SHAPES_3D = [(8, 8, 8), (16, 12, 10), (5, 7, 9), (1, 16, 4), (32, 1, 24), (48, 64, 80),
-             (3, 128, 2), (64, 64, 64), (96, 40, 30), (13, 11, 7)]
+             (3, 128, 2), (64, 64, 64), (96, 40, 30), (13, 11, 7), (17, 19, 23), (34, 31, 8)]
 
 
 @pytest.mark.parametrize("shape", SHAPES_3D)
@@ -125,8 +127,9 @@ def test_unknown_transform_and_bad_args():
         dfft.get_or_create_gpu_plan("not a tag", g, (1,))
     with pytest.raises(dfft.ArgumentError):
         dfft.fft(g, dims=(3,))
-    with pytest.raises(dfft.ArgumentError, match="prime factor"):
-        dfft.fft(torch.zeros((17 * 19,), dtype=torch.complex64, device="cuda"), dims=(1,))
+    # a prime length beyond what one CTA can convolve is rejected, not faked
+    with pytest.raises(dfft.ArgumentError):
+        dfft.fft(torch.zeros((32771,), dtype=torch.complex64, device="cuda"), dims=(1,))
 
 
 @pytest.mark.parametrize("shape", [(512, 64, 48), (64, 512, 8), (96, 96, 96), (256, 8, 512)])

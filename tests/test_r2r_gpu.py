@@ -14,13 +14,9 @@ KINDS = [dfft.REDFT10, dfft.REDFT01, dfft.REDFT11, dfft.RODFT10, dfft.RODFT01, d
 
 
 @pytest.mark.parametrize("kind", KINDS)
-@pytest.mark.parametrize("n", [2, 3, 4, 5, 8, 9, 16, 31, 64, 100, 256])
+@pytest.mark.parametrize("n", [2, 3, 4, 5, 8, 9, 16, 31, 64, 100, 256, 257])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_r2r_1d(kind, n, dtype):
-    if kind == dfft.REDFT00 and not _smooth(2 * (n - 1)):
-        pytest.skip("REDFT00 length 2(n-1) not 13-smooth")
-    if kind == dfft.RODFT00 and not _smooth(2 * (n + 1)):
-        pytest.skip("RODFT00 length 2(n+1) not 13-smooth")
     a = rand((n, 3), dtype, seed=kind * 1000 + n)
     y = dfft.fft(to_gpu(a), dims=(1,), transforms=(dfft.R2R((kind,)),))
     ref = oracle.r2r_direct(a.astype(np.longdouble), kind, 0)

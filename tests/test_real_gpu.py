@@ -10,7 +10,8 @@ from helpers import rand, rel, to_gpu, to_np, tol_for
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 6, 7, 8, 9, 15, 16, 30, 31, 64, 96, 100, 127, 128, 255, 256, 500, 512, 1024, 2048])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 6, 7, 8, 9, 15, 16, 30, 31, 34, 64, 96, 100, 127, 128,
+                               255, 256, 500, 512, 1024, 1018, 2048])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_rfft_irfft_1d(n, dtype):
     a = rand((n, 4), dtype, seed=n)
@@ -24,7 +25,8 @@ def test_rfft_irfft_1d(n, dtype):
     assert rel(to_np(x), oracle.irfft(ref, n, dims=(1,))) <= tol_for(dtype)
 
 
-@pytest.mark.parametrize("shape", [(16, 8, 4), (15, 6, 5), (64, 32, 48), (9, 10, 11), (256, 16, 8)])
+@pytest.mark.parametrize("shape", [(16, 8, 4), (15, 6, 5), (64, 32, 48), (9, 10, 11), (256, 16, 8),
+                                   (34, 17, 6)])
 @pytest.mark.parametrize("dims", [(1, 2, 3), (2, 3), (3, 1, 2), (1,), (2,)])
 @pytest.mark.parametrize("order", ["F", "C"])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
