@@ -1,0 +1,183 @@
+// Batches of independent transforms of uneven shapes, replayed as one CUDA
+// graph launch.
+//
+// A batch holds N plans (any shapes, kinds and precisions).  The first
+// execute with a given set of buffers captures every plan's passes into a
+// graph: the plans are spread over up to kBatchStreams forked capture
+// streams, so transforms of different grids become independent branches the
+// GPU runs concurrently (the persistent pipelined kernels of one branch and
+// the one-tile kernels of another share the SMs).  Later executes with the
+// same buffers replay the instantiated graph with one cudaGraphLaunch; new
+// buffers update the executable graph in place (cudaGraphExecUpdate) or,
+// if the topology changed, re-instantiate it.  Capture happens on a private
+// stream (capturing the legacy default stream is not allowed); the graph is
+// launched on the caller's stream.
+#include <cstring>
+#include <mutex>
+#include <vector>
+#include "dfft.h"
+#include "dfft_plan.h"
+
+namespace dfft {
+
+constexpr int kBatchStreams = 8;
+
+struct Batch {
+  int device = 0;
+  std::vector<Plan*> plans;       // not owned
+  std::vector<const void*> last_in;
+  std::vector<void*> last_out;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t side[kBatchStreams] = {};
+  cudaStream_t cap = nullptr;     // capture origin (the caller's stream may be the legacy one)
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kBatchStreams] = {};
+  int launches = 0;
+  std::mutex mu;
+  ~Batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (auto& s : side)
+      if (s) cudaStreamDestroy(s);
+    if (cap) cudaStreamDestroy(cap);
+    for (auto& e : join)
+      if (e) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+  }
+};
+
+// Records the batch into a graph on the batch's own capture stream (nothing
+// runs; the graph is launched on the caller's stream afterwards).
+static void capture(Batch* B, const void* const* ins, void* const* outs, cudaGraph_t* g) {
+  cudaStream_t s = B->cap;
+  const int n = (int)B->plans.size();
+  const int k = n < kBatchStreams ? n : kBatchStreams;
+  cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  cudaError_t err = cudaSuccess;
+  try {
+    cuda_check(cudaEventRecord(B->fork, s), "cudaEventRecord(fork)");
+    for (int i = 0; i < k; ++i) cuda_check(cudaStreamWaitEvent(B->side[i], B->fork, 0), "cudaStreamWaitEvent");
+    for (int i = 0; i < n; ++i) execute_plan(B->plans[i], ins[i], outs[i], B->side[i % k]);
+    for (int i = 0; i < k; ++i) {
+      cuda_check(cudaEventRecord(B->join[i], B->side[i]), "cudaEventRecord(join)");
+      cuda_check(cudaStreamWaitEvent(s, B->join[i], 0), "cudaStreamWaitEvent(join)");
+    }
+  } catch (...) {
+    cudaGraph_t dead = nullptr;
+    cudaStreamEndCapture(s, &dead);
+    if (dead) cudaGraphDestroy(dead);
+    cudaGetLastError();
+    throw;
+  }
+  err = cudaStreamEndCapture(s, g);
+  cuda_check(err, "cudaStreamEndCapture");
+}
+
+Batch* build_batch(int n, const dfft_plan* plans) {
+  if (n < 1 || !plans) throw Error{DFFT_ERROR_INVALID_VALUE, "a batch needs at least one plan"};
+  std::unique_ptr<Batch> B(new Batch());
+  cuda_check(cudaGetDevice(&B->device), "cudaGetDevice");
+  for (int i = 0; i < n; ++i) {
+    if (!plans[i] || !plans[i]->impl) throw Error{DFFT_ERROR_INVALID_VALUE, "NULL plan in batch"};
+    if (plans[i]->impl->device != B->device)
+      throw Error{DFFT_ERROR_INVALID_VALUE, "every plan of a batch must live on the current device"};
+    B->plans.push_back(plans[i]->impl);
+    B->launches += (int)plans[i]->impl->passes.size();
+  }
+  for (auto& s : B->side) cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+  cuda_check(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (auto& e : B->join) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  cuda_check(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming), "cudaEventCreate");
+  return B.release();
+}
+
+void execute_batch(Batch* B, const void* const* ins, void* const* outs, cudaStream_t s) {
+  if (!ins || !outs) throw Error{DFFT_ERROR_INVALID_VALUE, "ins/outs is NULL"};
+  std::lock_guard<std::mutex> lk(B->mu);
+  const int n = (int)B->plans.size();
+  for (int i = 0; i < n; ++i)
+    if (!ins[i] || !outs[i]) throw Error{DFFT_ERROR_INVALID_VALUE, "NULL buffer in batch"};
+  int cur = -1;
+  cuda_check(cudaGetDevice(&cur), "cudaGetDevice");
+  if (cur != B->device) cuda_check(cudaSetDevice(B->device), "cudaSetDevice");
+  bool same = B->exec && (int)B->last_in.size() == n;
+  for (int i = 0; same && i < n; ++i) same = B->last_in[i] == ins[i] && B->last_out[i] == outs[i];
+  if (!same) {
+    cudaGraph_t g = nullptr;
+    capture(B, ins, outs, &g);
+    bool updated = false;
+    if (B->exec) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(B->exec, g, &info) == cudaSuccess) updated = true;
+      else cudaGetLastError();
+    }
+    if (!updated) {
+      if (B->exec) cudaGraphExecDestroy(B->exec);
+      B->exec = nullptr;
+      cudaError_t e = cudaGraphInstantiate(&B->exec, g, 0);
+      cudaGraphDestroy(g);
+      cuda_check(e, "cudaGraphInstantiate");
+    } else {
+      cudaGraphDestroy(g);
+    }
+    B->last_in.assign(ins, ins + n);
+    B->last_out.assign(outs, outs + n);
+  }
+  cudaError_t e = cudaGraphLaunch(B->exec, s);
+  if (cur != B->device) cudaSetDevice(cur);
+  cuda_check(e, "cudaGraphLaunch");
+}
+
+}  // namespace dfft
+
+struct dfft_batch_s {
+  dfft::Batch* impl;
+};
+
+using dfft::Error;
+
+extern "C" {
+
+int dfft_batch_create(dfft_batch* batch, int nplans, const dfft_plan* plans) {
+  try {
+    if (!batch) throw Error{DFFT_ERROR_INVALID_VALUE, "batch is NULL"};
+    *batch = nullptr;
+    *batch = new dfft_batch_s{dfft::build_batch(nplans, plans)};
+    return DFFT_SUCCESS;
+  } catch (const Error& e) {
+    dfft::set_error(e.msg);
+    return e.status;
+  } catch (...) {
+    dfft::set_error("unexpected exception");
+    return DFFT_ERROR_INVALID_VALUE;
+  }
+}
+
+int dfft_batch_execute(dfft_batch batch, const void* const* ins, void* const* outs, void* stream) {
+  try {
+    if (!batch || !batch->impl) throw Error{DFFT_ERROR_INVALID_VALUE, "batch is NULL"};
+    dfft::execute_batch(batch->impl, ins, outs, reinterpret_cast<cudaStream_t>(stream));
+    return DFFT_SUCCESS;
+  } catch (const Error& e) {
+    dfft::set_error(e.msg);
+    return e.status;
+  }
+}
+
+int dfft_batch_launches(dfft_batch batch, int* launches) {
+  if (!batch || !batch->impl || !launches) {
+    dfft::set_error("NULL argument");
+    return DFFT_ERROR_INVALID_VALUE;
+  }
+  *launches = batch->impl->launches;
+  return DFFT_SUCCESS;
+}
+
+int dfft_batch_destroy(dfft_batch batch) {
+  if (batch) {
+    delete batch->impl;
+    delete batch;
+  }
+  return DFFT_SUCCESS;
+}
+
+}  // extern "C"

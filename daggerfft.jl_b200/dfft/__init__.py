@@ -7,7 +7,7 @@ the reference's Julia API.
 """
 from ._lib import (FLAG_DESTROY_INPUT, FLAG_NO_WISDOM, FLAG_TUNE, ArgumentError, DFFTError, LIB_PATH,
                    device_error, lib, wisdom_export, wisdom_forget, wisdom_import, wisdom_size)
-from .api import (DHT, FFT, FFT_, GPU_PLAN_CACHE, HC2R, IFFT, IFFT_, IRFFT, IRFFT_, R2HC, R2R,
+from .api import (Batch, DHT, FFT, FFT_, GPU_PLAN_CACHE, HC2R, IFFT, IFFT_, IRFFT, IRFFT_, R2HC, R2R,
                   R2R_SUPPORTED_KINDS, REDFT00, REDFT01, REDFT10, REDFT11, RFFT, RFFT_, RODFT00,
                   RODFT01, RODFT10, RODFT11, Decomposition, Pencil, Plan, Slab, Transform,
                   apply_gpu_fft_, empty_like_layout, fft, fft_, get_or_create_gpu_plan,

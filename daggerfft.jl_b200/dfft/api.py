@@ -393,3 +393,56 @@ def ifft_(A, decomp=None, dims=(1, 2, 3), method="plain"):
         raise ArgumentError(_lib.ERROR_INVALID_VALUE, "ifft! needs a contiguous array")
     p = get_or_create_gpu_plan(IFFT_(), A, _norm_dims(dims, A.dim()), decomp=decomp, method=method)
     return p.execute(A, A)
+
+
+# ---------------------------------------------------------------------------
+# batches of uneven transforms (one CUDA graph launch)
+# ---------------------------------------------------------------------------
+
+
+class Batch:
+    """Independent plans executed together as one CUDA graph launch
+    (``dfft_batch_*``).  ``execute(ins, outs)`` takes one input and one
+    output tensor per plan; the graph is captured on the first call and
+    replayed while the same buffers are passed."""
+
+    def __init__(self, plans: Sequence[Plan]):
+        L = _lib.lib()
+        self._L = L
+        self.plans = list(plans)  # keeps the plans alive
+        L.dfft_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_void_p)]
+        L.dfft_batch_create.restype = ctypes.c_int
+        L.dfft_batch_execute.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                         ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]
+        L.dfft_batch_execute.restype = ctypes.c_int
+        L.dfft_batch_launches.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        L.dfft_batch_launches.restype = ctypes.c_int
+        L.dfft_batch_destroy.argtypes = [ctypes.c_void_p]
+        L.dfft_batch_destroy.restype = ctypes.c_int
+        arr = (ctypes.c_void_p * len(self.plans))(*[p._h.value for p in self.plans])
+        h = ctypes.c_void_p()
+        check(L.dfft_batch_create(ctypes.byref(h), len(self.plans), arr))
+        self._h = h
+        n = ctypes.c_int()
+        check(L.dfft_batch_launches(h, ctypes.byref(n)))
+        self.launches = n.value
+
+    def execute(self, ins, outs, stream=None):
+        if len(ins) != len(self.plans) or len(outs) != len(self.plans):
+            raise ArgumentError(_lib.ERROR_INVALID_VALUE, "one input and one output per plan")
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        ia = (ctypes.c_void_p * len(ins))(*[t.data_ptr() for t in ins])
+        oa = (ctypes.c_void_p * len(outs))(*[t.data_ptr() for t in outs])
+        check(self._L.dfft_batch_execute(self._h, ia, oa, ctypes.c_void_p(stream.cuda_stream)))
+        return outs
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._L.dfft_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None

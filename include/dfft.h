@@ -153,6 +153,22 @@ DFFT_API int dfft_wisdom_import(const char* path);
 DFFT_API int dfft_wisdom_forget(void);
 DFFT_API int dfft_wisdom_size(int* n);
 
+/* ---- batches of uneven transforms -----------------------------------
+ *
+ * No counterpart in the reference (north-star addition): N independent
+ * plans (any shapes/kinds) executed as one CUDA graph launch.  The first
+ * execute with a set of buffers captures every plan's passes as concurrent
+ * branches; later executes with the same buffers replay the graph, new
+ * buffers update it.  Plans must outlive the batch and live on the current
+ * device.
+ */
+typedef struct dfft_batch_s* dfft_batch;
+DFFT_API int dfft_batch_create(dfft_batch* batch, int nplans, const dfft_plan* plans);
+DFFT_API int dfft_batch_execute(dfft_batch batch, const void* const* ins, void* const* outs,
+                                void* stream);
+DFFT_API int dfft_batch_launches(dfft_batch batch, int* launches);
+DFFT_API int dfft_batch_destroy(dfft_batch batch);
+
 /* ---- redistribution between blockings --------------------------------
  *
  * One sub-block copy: `count` elements per dim from chunk `src` (column-major
