@@ -7,6 +7,13 @@
       {48,64,80,96,120,128,160,192}, uniform [-1,1), as one graph launch
       (dfft.Batch) vs the same plans launched one after another; plus the
       2-D DCT-II/III Float64 256x256x32 stack.
+  c5  serving: Poisson arrivals at swept rates into dfft.Server; each
+      request a forward or inverse 3-D FFT (C2C ComplexF32 / ComplexF64 or
+      R2C Float32) with cubic edge from {64,96,128,192,256,384} (weights
+      30/20/20/15/10/5 %), standard-normal inputs from per-request seeds
+      (a pool of resident inputs per kind and edge); results stay in the
+      server arena and are released on completion; p50/p99 latency and
+      throughput per rate.
 
 Usage: python daggerfft.jl_b200/bench_configs.py [c1 c2 c4 ...]
 Times are CUDA-event averages after warm-up; bytes are algorithmic (one
@@ -135,6 +142,83 @@ def c4():
                       "dct2_dct3_256x256x32_f64_ms": round(ms_dct, 4),
                       "dct_GBps": round(dbytes / ms_dct / 1e6, 1),
                       "dct_roundtrip_rel_l2": err}), flush=True)
+
+
+def c5(rates=(250, 500, 1000, 2000, 4000), seconds=2.0, budget=16 << 30, slots=8):
+    import random
+    edges = [64, 96, 128, 192, 256, 384]
+    weights = [30, 20, 20, 15, 10, 5]
+    kinds = ["c2c32", "c2c64", "r2c32"]
+    pool = {}
+    g = torch.Generator(device="cuda").manual_seed(5)
+    for k in kinds:
+        for e in edges:
+            vs = []
+            for v in range(2):
+                if k == "c2c32":
+                    fwd_in = fcol(torch.randn((e, e, e), device="cuda", dtype=torch.complex64, generator=g))
+                    inv_in = fwd_in
+                elif k == "c2c64":
+                    fwd_in = fcol(torch.randn((e, e, e), device="cuda", dtype=torch.complex128, generator=g))
+                    inv_in = fwd_in
+                else:
+                    fwd_in = fcol(torch.randn((e, e, e), device="cuda", dtype=torch.float32, generator=g))
+                    inv_in = dfft.rfft(fwd_in)
+                vs.append((fwd_in, inv_in))
+            pool[(k, e)] = vs
+    srv = dfft.Server(budget, slots=slots)
+
+    def submit(k, e, fwd, v):
+        a_f, a_i = pool[(k, e)][v]
+        if k == "r2c32":
+            return srv.submit(dfft.RFFT(), a_f) if fwd else srv.submit(dfft.IRFFT(), a_i, n=e)
+        return srv.submit(dfft.FFT() if fwd else dfft.IFFT(), a_f if fwd else a_i)
+
+    # plans resident before timing: every kind/edge/direction `slots` times
+    # at once, so plans that need one instance per running request exist
+    warm = [submit(k, e, f, 0) for k in kinds for e in edges for f in (True, False) for _ in range(slots)]
+    for rid in warm:
+        srv.wait(rid, 60000)
+        srv.release(rid)
+    srv.poll()  # drop the warm-up ids from the finished list
+    results = []
+    rng = random.Random(7)
+    for lam in rates:
+        srv.reset_stats()
+        t_end = time.perf_counter() + seconds
+        t_next = time.perf_counter()
+        outstanding = set()
+        n_sub = 0
+        while True:
+            now = time.perf_counter()
+            if now >= t_end:
+                break
+            while t_next <= now:
+                e = rng.choices(edges, weights)[0]
+                k = kinds[rng.randrange(3)]
+                outstanding.add(submit(k, e, rng.random() < 0.5, rng.randrange(2)))
+                n_sub += 1
+                t_next += rng.expovariate(lam)
+            for rid in srv.poll():
+                if rid in outstanding:
+                    srv.release(rid)
+                    outstanding.discard(rid)
+            time.sleep(0.0002)
+        for rid in list(outstanding):
+            srv.wait(rid, 120000)
+            srv.release(rid)
+        srv.poll()
+        st = srv.stats()
+        results.append({"rate_req_per_s": lam, "submitted": n_sub, "completed": st["completed"],
+                        "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+                        "max_ms": round(st["max_ms"], 3),
+                        "throughput_req_per_s": round(st["completed"] / st["elapsed_s"], 1),
+                        "io_GBps": round(st["bytes_moved"] / st["elapsed_s"] / 1e9, 2),
+                        "peak_running": st["peak_running"], "arena_peak_GB": round(st["arena_peak_bytes"] / 1e9, 2)})
+    print(json.dumps({"config": "c5 serving, Poisson arrivals, mixed fft/ifft/rfft/irfft",
+                      "slots": slots, "hbm_budget_GB": budget / 1e9, "seconds_per_rate": seconds,
+                      "rates": results}), flush=True)
+    srv.close()
 
 
 if __name__ == "__main__":

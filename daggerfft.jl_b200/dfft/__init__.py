@@ -17,4 +17,6 @@ from .darray import (Blocks, CudaCopier, DArray, Workspace, collect, compute_ove
                      create_gpu_workspace, distribute, empty_darray, gpu_cleanup_workspace_,
                      gpu_coalesced_redistribute_, gpu_fft_, gpu_ifft_)
 
+from .serve import Server
+
 __version__ = "0.1.0"

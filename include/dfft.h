@@ -169,6 +169,63 @@ DFFT_API int dfft_batch_execute(dfft_batch batch, const void* const* ins, void* 
 DFFT_API int dfft_batch_launches(dfft_batch batch, int* launches);
 DFFT_API int dfft_batch_destroy(dfft_batch batch);
 
+/* ---- serving: continuous batching of transform requests --------------
+ *
+ * No counterpart in the reference (north-star addition).  A server owns an
+ * HBM arena of `hbm_budget_bytes` (allocated once) and `slots` execution
+ * streams.  Requests are admitted in arrival order while a slot is free and
+ * their staging memory (host input copied in, host or server-held output)
+ * fits the arena; admitted requests run concurrently on their own streams
+ * and new ones join as slots and memory free up.  Plans, twiddles and
+ * workspaces stay resident per shape.  Every request must be released
+ * (dfft_server_release) after it finishes.
+ */
+enum { DFFT_MEM_DEVICE = 0, DFFT_MEM_HOST = 1, DFFT_MEM_SERVER = 2 };
+
+typedef struct {
+  int transform;          /* DFFT_FFT, DFFT_IFFT, DFFT_RFFT, DFFT_IRFFT, DFFT_R2R ... */
+  int precision;          /* DFFT_F32 / DFFT_F64 */
+  int decomp;             /* DFFT_PENCIL / DFFT_SLAB */
+  int ndim;
+  int64_t shape[3];       /* input shape, column-major */
+  int ndims;
+  int32_t dims[3];        /* 1-based */
+  int32_t r2r_kinds[3];
+  int64_t irfft_len;
+  const void* in;
+  int in_location;        /* DFFT_MEM_DEVICE or DFFT_MEM_HOST (pinned for overlap) */
+  void* out;              /* ignored for DFFT_MEM_SERVER */
+  int out_location;       /* DFFT_MEM_DEVICE, DFFT_MEM_HOST or DFFT_MEM_SERVER */
+} dfft_request;
+
+typedef struct {
+  uint64_t completed, rejected, cancelled, failed, queued;
+  double p50_ms, p99_ms, max_ms;   /* submit -> completion latency */
+  double bytes_moved;              /* input + output bytes of completed requests */
+  double elapsed_s;                /* since creation or the last reset */
+  size_t arena_bytes, arena_peak_bytes;
+  int peak_running;                /* most requests on the GPU at once */
+  int resident_plans;
+} dfft_server_stats;
+
+typedef struct dfft_server_s* dfft_server;
+
+DFFT_API int dfft_server_create(dfft_server* server, size_t hbm_budget_bytes, int slots, unsigned flags);
+DFFT_API int dfft_server_submit(dfft_server server, const dfft_request* req, uint64_t* id);
+/* ids of finished (completed, failed or cancelled) requests, oldest first */
+DFFT_API int dfft_server_poll(dfft_server server, uint64_t* ids, int max, int* n);
+/* bounded wait for one request; status = its result (DFFT_ERROR_TIMEOUT if not done) */
+DFFT_API int dfft_server_wait(dfft_server server, uint64_t id, int timeout_ms, int* status);
+/* copy a server-held result out (DFFT_MEM_HOST or DFFT_MEM_DEVICE destination) */
+DFFT_API int dfft_server_fetch(dfft_server server, uint64_t id, void* dst, int dst_location, void* stream);
+DFFT_API int dfft_server_result_pointer(dfft_server server, uint64_t id, void** ptr);
+DFFT_API int dfft_server_release(dfft_server server, uint64_t id);
+/* cancel a request that has not been admitted yet */
+DFFT_API int dfft_server_cancel(dfft_server server, uint64_t id);
+DFFT_API int dfft_server_get_stats(dfft_server server, dfft_server_stats* stats);
+DFFT_API int dfft_server_reset_stats(dfft_server server);
+DFFT_API int dfft_server_destroy(dfft_server server);
+
 /* ---- redistribution between blockings --------------------------------
  *
  * One sub-block copy: `count` elements per dim from chunk `src` (column-major
