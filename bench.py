@@ -182,12 +182,13 @@ def run_profile(args):
     a = torch.randn(tuple(reversed(shape)), dtype=torch.complex64, device="cuda", generator=g)
     A = a.permute(*reversed(range(len(shape))))
     B = dfft.empty_like_layout(A.shape, A.dtype, A)
-    p = dfft.gpu_plan_transform(dfft.FFT(), A, (args.profile,), method=args.method,
-                                flags=0 if args.no_tune else dfft.FLAG_TUNE)
+    dims = tuple(int(c) for c in args.profile)
+    flags = (0 if args.no_tune else dfft.FLAG_TUNE) | (dfft.FLAG_NO_FUSE if args.no_fuse else 0)
+    p = dfft.gpu_plan_transform(dfft.FFT(), A, dims, method=args.method, flags=flags)
     for _ in range(2):
         p.execute(A, B)
     torch.cuda.synchronize()
-    print(f"profile: dim {args.profile} of {shape}, {p.launches} launch(es) per call, 2 calls")
+    print(f"profile: dims {dims} of {shape}, {p.launches} launch(es) per call, 2 calls")
 
 
 def main():
@@ -199,8 +200,11 @@ def main():
     ap.add_argument("--method", default="plain", choices=["plain", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="heuristic launch shapes, no autotuning")
-    ap.add_argument("--profile", type=int, default=0,
-                    help="profiling mode: run 2 launches of the pass along this dim (1-3) and exit")
+    ap.add_argument("--profile", default="",
+                    help="profiling mode: run the plan over these dims twice and exit "
+                         "(e.g. 1 = the dim-1 pass, 12 = the fused dims-(1,2) slab pass)")
+    ap.add_argument("--no-fuse", action="store_true",
+                    help="one pass per axis (no fused dims-(1,2) slab pass)")
     ap.add_argument("--shape", default="512,512,512", help="profiling mode: ComplexF32 array shape")
     args = ap.parse_args()
     if args.profile:
@@ -236,7 +240,7 @@ def main():
     Bd = dfft.empty_like_layout(Ad.shape, Ad.dtype, Ad)
     Cd = dfft.empty_like_layout(Ad.shape, Ad.dtype, Ad)
     decomp = dfft.Slab()
-    flags = 0 if args.no_tune else dfft.FLAG_TUNE
+    flags = (0 if args.no_tune else dfft.FLAG_TUNE) | (dfft.FLAG_NO_FUSE if args.no_fuse else 0)
     pf = dfft.get_or_create_gpu_plan(dfft.FFT(), Ad, (1, 2, 3), decomp=decomp, method=args.method,
                                      flags=flags)
     pi = dfft.get_or_create_gpu_plan(dfft.IFFT(), Bd, (1, 2, 3), decomp=decomp, method=args.method,

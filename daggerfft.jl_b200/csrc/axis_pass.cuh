@@ -285,23 +285,27 @@ __device__ __forceinline__ void store_elem(const IoAny& io, long long b, int k,
 // Shared-memory view of one column.  PadCol: column-major with one pad
 // element per 128 bytes (direct-load kernels); StrideCol: the [k][c] layout a
 // TMA tile box lands in (c fastest), conflict-free for the cfast mapping.
+// Every view is addressed as (base, off): element base + off, where the
+// stage passes its per-butterfly index as base and r * stride (a constant
+// once the radix loop is unrolled) as off.  Views whose layout is a bitwise
+// map use it to split the address into a per-butterfly part and a constant.
 template <typename V> struct PadCol {
   V* p;
-  __device__ __forceinline__ V ld(int k) const { return p[swz<V>(k)]; }
-  __device__ __forceinline__ void st(int k, V v) const { p[swz<V>(k)] = v; }
+  __device__ __forceinline__ V ld(int b, int off) const { return p[swz<V>(b + off)]; }
+  __device__ __forceinline__ void st(int b, int off, V v) const { p[swz<V>(b + off)] = v; }
 };
 template <typename V> struct StrideCol {
   V* p;
   int s;
-  __device__ __forceinline__ V ld(int k) const { return p[k * s]; }
-  __device__ __forceinline__ void st(int k, V v) const { p[k * s] = v; }
+  __device__ __forceinline__ V ld(int b, int off) const { return p[(b + off) * s]; }
+  __device__ __forceinline__ void st(int b, int off, V v) const { p[(b + off) * s] = v; }
 };
 // StrideCol with a compile-time stride: every tile offset becomes an
 // immediate of the shared-memory instruction instead of a live register.
 template <typename V, int S> struct StrideColC {
   V* p;
-  __device__ __forceinline__ V ld(int k) const { return p[k * S]; }
-  __device__ __forceinline__ void st(int k, V v) const { p[k * S] = v; }
+  __device__ __forceinline__ V ld(int b, int off) const { return p[(b + off) * S]; }
+  __device__ __forceinline__ void st(int b, int off, V v) const { p[(b + off) * S] = v; }
 };
 
 // Twiddle sources.  GlobalTw reads w_L^{jm*r*ts} from the L-entry table;
@@ -342,22 +346,31 @@ template <typename V> struct StageTwG {
   }
 };
 
+// Barrier between the stages: the whole CTA (BAR = 0) or named barrier 1
+// over the BAR threads that run the stages (the other warps of the CTA do
+// something else, e.g. feed the tile pipeline).
+template <int BAR> __device__ __forceinline__ void stage_sync() {
+  if constexpr (BAR == 0) __syncthreads();
+  else asm volatile("bar.sync 1, %0;" ::"n"(BAR) : "memory");
+}
+
 // BMAX: upper bound on butterflies per thread; in the static kernels it is
 // exactly ceil((L/R)/P), in the dynamic kernel EMAX/R.
-// SMEM_IO: the first stage reads and the last stage writes shared memory
-// (pipelined kernels) instead of global memory.
+// SMEM_IO: 0 = the first stage reads and the last stage writes global
+// memory; 1 = both go through shared memory (pipelined kernels); 2 = the
+// first stage reads shared memory, the last stage writes global memory.
 // CIN/COUT: the shared-memory views the stage reads and writes (they differ
 // when a stage moves a tile between a dense TMA buffer and a padded one).
 // toff: offset of this stage in a StageTw table (Ns - R_0).
-template <typename T, int R, int BMAX, bool FAST_IO, bool SMEM_IO, class CIN, class COUT, class TW>
+template <typename T, int R, int BMAX, bool FAST_IO, int SMEM_IO, int BAR, class CIN, class COUT, class TW>
 __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int Ns, int ts, int toff,
                                            bool first, bool last, int t, const CIN& cin,
                                            const COUT& cout, const TW& tw, long long ib,
                                            long long ob, bool cv) {
   typedef typename cvec<T>::type V;
   const int Lr = L / R;
-  const bool to_global = !SMEM_IO && last && !d.epi;
-  const bool from_global = !SMEM_IO && first;
+  const bool to_global = SMEM_IO != 1 && last && !d.epi;
+  const bool from_global = SMEM_IO == 0 && first;
   V v[BMAX][R];
 #pragma unroll
   for (int b = 0; b < BMAX; ++b) {
@@ -374,14 +387,14 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
           if (d.inverse) x.y = -x.y;
           v[b][r] = x;
         } else {
-          V x = cin.ld(k);
-          if (SMEM_IO && first && d.inverse) x.y = -x.y;
+          V x = cin.ld(j, r * Lr);
+          if (SMEM_IO != 0 && first && d.inverse) x.y = -x.y;
           v[b][r] = x;
         }
       }
     }
   }
-  if (!from_global) __syncthreads();
+  if (!from_global) stage_sync<BAR>();
 #pragma unroll
   for (int b = 0; b < BMAX; ++b) {
     const int j = t + b * P;
@@ -400,20 +413,21 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
           if (cv) {
             V y = v[b][r];
             if (d.inverse) y.y = -y.y;
-            if (FAST_IO) reinterpret_cast<V*>(d.out.p)[ob + k * d.out.sk] = cscale(y, (T)d.scale);
+            // SMEM_IO 2 (the fused slab pass) stores whole pencils: unit stride
+            if (FAST_IO) reinterpret_cast<V*>(d.out.p)[ob + (SMEM_IO == 2 ? k : k * d.out.sk)] = cscale(y, (T)d.scale);
             else store_elem<T>(d.out, ob, k, y, (T)d.scale);
           }
-        } else if (SMEM_IO && last) {
+        } else if (SMEM_IO == 1 && last) {
           V y = v[b][r];
           if (d.inverse) y.y = -y.y;
-          cout.st(k, cscale(y, (T)d.scale));
+          cout.st(o0, r * Ns, cscale(y, (T)d.scale));
         } else {
-          cout.st(k, v[b][r]);
+          cout.st(o0, r * Ns, v[b][r]);
         }
       }
     }
   }
-  if (!to_global) __syncthreads();
+  if (!to_global) stage_sync<BAR>();
 }
 
 // Shared prologue: thread -> (column, butterfly lane), column base offsets.
@@ -461,7 +475,7 @@ __device__ __forceinline__ void r2c_epilogue(const PassDesc& d, int P, const Col
 
 // Compile-time stage sequence.  The first stage reads CFIRST, the last
 // stage writes CLAST, every other access goes through CMID.
-template <typename T, int L, int P, bool FAST_IO, bool SMEM_IO, int NS, int R0, int S, class CFIRST,
+template <typename T, int L, int P, bool FAST_IO, int SMEM_IO, int BAR, int NS, int R0, int S, class CFIRST,
           class CMID, class CLAST, class TW, int R, int... Rest>
 __device__ __forceinline__ void static_stages(const PassDesc& d, int t, const CFIRST& cf,
                                               const CMID& cm, const CLAST& cl, const TW& tw,
@@ -473,16 +487,16 @@ __device__ __forceinline__ void static_stages(const PassDesc& d, int t, const CF
   constexpr bool LAST = (sizeof...(Rest) == 0);
   constexpr int R0_ = FIRST ? R : R0;
   if constexpr (FIRST && LAST) {
-    stage_body<T, R, BM, FAST_IO, SMEM_IO>(d, L, P, NS, TS, NS - R0_, true, true, t, cf, cl, tw, ib, ob, cv);
+    stage_body<T, R, BM, FAST_IO, SMEM_IO, BAR>(d, L, P, NS, TS, NS - R0_, true, true, t, cf, cl, tw, ib, ob, cv);
   } else if constexpr (FIRST) {
-    stage_body<T, R, BM, FAST_IO, SMEM_IO>(d, L, P, NS, TS, NS - R0_, true, false, t, cf, cm, tw, ib, ob, cv);
+    stage_body<T, R, BM, FAST_IO, SMEM_IO, BAR>(d, L, P, NS, TS, NS - R0_, true, false, t, cf, cm, tw, ib, ob, cv);
   } else if constexpr (LAST) {
-    stage_body<T, R, BM, FAST_IO, SMEM_IO>(d, L, P, NS, TS, NS - R0_, false, true, t, cm, cl, tw, ib, ob, cv);
+    stage_body<T, R, BM, FAST_IO, SMEM_IO, BAR>(d, L, P, NS, TS, NS - R0_, false, true, t, cm, cl, tw, ib, ob, cv);
   } else {
-    stage_body<T, R, BM, FAST_IO, SMEM_IO>(d, L, P, NS, TS, NS - R0_, false, false, t, cm, cm, tw, ib, ob, cv);
+    stage_body<T, R, BM, FAST_IO, SMEM_IO, BAR>(d, L, P, NS, TS, NS - R0_, false, false, t, cm, cm, tw, ib, ob, cv);
   }
   if constexpr (sizeof...(Rest) > 0)
-    static_stages<T, L, P, FAST_IO, SMEM_IO, NS * R, R0_, S + 1, CFIRST, CMID, CLAST, TW, Rest...>(
+    static_stages<T, L, P, FAST_IO, SMEM_IO, BAR, NS * R, R0_, S + 1, CFIRST, CMID, CLAST, TW, Rest...>(
         d, t, cf, cm, cl, tw, ib, ob, cv);
 }
 
@@ -494,7 +508,7 @@ __global__ void __launch_bounds__(LB) axis_pass_static(const PassDesc d) {
   const ColCtx x = col_ctx(d, P);
   const PadCol<V> col{sm + x.c * d.ld};
   const GlobalTw<V> tw{reinterpret_cast<const V*>(d.tw)};
-  static_stages<T, L, P, FAST_IO, false, 1, 1, 0, PadCol<V>, PadCol<V>, PadCol<V>, GlobalTw<V>, Rs...>(
+  static_stages<T, L, P, FAST_IO, 0, 0, 1, 1, 0, PadCol<V>, PadCol<V>, PadCol<V>, GlobalTw<V>, Rs...>(
       d, x.t, col, col, col, tw, x.ib, x.ob, x.cv);
   if (!FAST_IO && d.epi) r2c_epilogue<T>(d, P, x, col.p);
 }
@@ -511,11 +525,11 @@ __device__ __noinline__ void dyn_stage(const PassDesc& d, int s, int t, typename
   const PadCol<V> c{col};
   if constexpr (CTW) {
     const ComputedTw<V> g{d.L};
-    stage_body<T, R, EMAX / R, false, false>(d, d.L, d.P, d.ns[s], d.tws[s], 0, s == 0,
+    stage_body<T, R, EMAX / R, false, 0, 0>(d, d.L, d.P, d.ns[s], d.tws[s], 0, s == 0,
                                              s == d.nst - 1, t, c, c, g, ib, ob, cv);
   } else {
     const GlobalTw<V> g{tw};
-    stage_body<T, R, EMAX / R, false, false>(d, d.L, d.P, d.ns[s], d.tws[s], 0, s == 0,
+    stage_body<T, R, EMAX / R, false, 0, 0>(d, d.L, d.P, d.ns[s], d.tws[s], 0, s == 0,
                                              s == d.nst - 1, t, c, c, g, ib, ob, cv);
   }
 }

@@ -56,7 +56,17 @@ static void capture(Batch* B, const void* const* ins, void* const* outs, cudaGra
   try {
     cuda_check(cudaEventRecord(B->fork, s), "cudaEventRecord(fork)");
     for (int i = 0; i < k; ++i) cuda_check(cudaStreamWaitEvent(B->side[i], B->fork, 0), "cudaStreamWaitEvent");
-    for (int i = 0; i < n; ++i) execute_plan(B->plans[i], ins[i], outs[i], B->side[i % k]);
+    // a plan listed more than once whose workspace is live during a launch
+    // (C2R scratch, slab-pass counters) runs its uses one after another on
+    // the branch of its first use
+    std::vector<int> branch(n);
+    for (int i = 0; i < n; ++i) {
+      branch[i] = i % k;
+      if (B->plans[i]->work_bytes)
+        for (int j = 0; j < i; ++j)
+          if (B->plans[j] == B->plans[i]) { branch[i] = branch[j]; break; }
+    }
+    for (int i = 0; i < n; ++i) execute_plan(B->plans[i], ins[i], outs[i], B->side[branch[i]]);
     for (int i = 0; i < k; ++i) {
       cuda_check(cudaEventRecord(B->join[i], B->side[i]), "cudaEventRecord(join)");
       cuda_check(cudaStreamWaitEvent(s, B->join[i], 0), "cudaStreamWaitEvent(join)");

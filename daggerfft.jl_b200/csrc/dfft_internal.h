@@ -5,7 +5,7 @@
 #include <memory>
 #include <string>
 #include <vector>
-#include "tma_pass.cuh"
+#include "slab_pass.cuh"
 
 namespace dfft {
 
@@ -50,8 +50,38 @@ struct Pass {
   bool tma = false;
   TmaGeom geom{};
   long long tI = 0, tL = 0, tO = 0;
+  // fused 2-D slab pass (dims 1 and 2 of an L x L x O array): d is the
+  // x-phase descriptor, d2 the y-phase one; tensor map as for tma with
+  // {tI, tL, tO} = {L, L, O} over the output
+  bool slab = false;
+  size_t ctr_bytes = 0;  // job and per-slab counters (in the plan workspace)
+  PassDesc d2{};
+  SlabGeom sgeom{};
   std::vector<std::shared_ptr<DevTable>> tables;
 };
+
+// A launch shape of the fused slab kernel (slab_pass.cu): tile width x
+// threads per pencil.  Variants of one (precision, L) are listed best-first
+// for the untuned planner.
+struct SlabKernel {
+  int dbl, L, P, nst, radix[4];
+  int lb;   // threads per CTA
+  int cs;   // pencils / columns per tile
+  const void* fn;
+};
+// Variant `v` (0-based) for (dbl, L), or null past the last one.
+const SlabKernel* find_slab_kernel(int dbl, int L, int v = 0);
+
+// Fused forward or inverse 2-D C2C over dims 1 and 2 of an L x L x O array
+// (scales: 1 forward, 1/L per axis inverse) with launch variant v; throws
+// Error{DFFT_ERROR_UNSUPPORTED_SIZE} when that variant cannot serve the shape.
+Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v = 0);
+
+// Fused variant to use for dims (1, 2) of an L x L x O array, or -1 for the
+// per-axis passes `split` (x then y, already planned): wisdom, then timing
+// under DFFT_FLAG_TUNE, else the first variant that builds.
+int choose_slab(int dbl, int L, long long O, int inverse, const std::vector<Pass>& split,
+                unsigned flags);
 
 // Device error word of the current device (bounded waits that expire set it).
 int* device_error_word();
@@ -89,8 +119,9 @@ int wisdom_import(const char* path);
 void wisdom_forget();
 int wisdom_size();
 
-// Launches one pass on `stream` with the given buffers.
-cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream);
+// Launches one pass on `stream` with the given buffers; `work` holds the
+// counters of a fused slab pass (p.ctr_bytes, zeroed here before the launch).
+cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream, void* work = nullptr);
 
 // Raise the dynamic shared-memory limit of a kernel on the current device.
 cudaError_t ensure_smem_attr(const void* fn, size_t bytes);

@@ -18,7 +18,7 @@ struct Plan {
   int64_t out_shape[3] = {1, 1, 1};
   size_t in_elem = 0, out_elem = 0;
   std::vector<Pass> passes;
-  void* work = nullptr;           // plan-owned workspace (C2R over several dims)
+  void* work = nullptr;           // plan-owned workspace (C2R over several dims, slab-pass counters)
   size_t work_bytes = 0;
   void* chirp = nullptr;          // Bluestein scratch (Q*M complex per axis, max over axes)
   size_t chirp_bytes = 0;

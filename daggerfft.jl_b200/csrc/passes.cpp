@@ -1,4 +1,5 @@
 // Pass construction: radix plan lookup, launch shape, twiddle tables.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -470,13 +471,120 @@ Pass make_pass(const PassSpec& s) {
   return p;
 }
 
-cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream) {
+Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v) {
+  const SlabKernel* k = find_slab_kernel(dbl, L, v);
+  if (!k) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "no fused slab kernel for this length"};
+  if (L % k->cs != 0) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "slab tiling does not divide L"};
+  const StaticPlan* sp = find_static(dbl, L);
+  if (!sp || sp->nst != k->nst || !std::equal(k->radix, k->radix + k->nst, sp->radix))
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "fused slab kernel and static plan disagree"};
+  if (O < 1 || O >= (1LL << 31)) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "slab count out of range"};
+  const int esz = dbl ? 16 : 8;
+  const std::vector<int> rad(k->radix, k->radix + k->nst);
+  Pass p;
+  p.slab = true;
+  p.is_static = true;
+  p.fn = k->fn;
+  int ld = swz_host(L - 1, esz) + 1;
+  if ((ld & 1) == 0) ld += 1;
+  auto fill = [&](PassDesc& d, long long I) {
+    d.L = L;
+    d.nst = k->nst;
+    int ns = 1;
+    for (int i = 0; i < d.nst; ++i) {
+      d.radix[i] = rad[i];
+      d.ns[i] = ns;
+      d.tws[i] = L / (ns * rad[i]);
+      ns *= rad[i];
+    }
+    d.P = k->P;
+    d.C = k->cs;
+    d.ld = ld;
+    d.inverse = inverse;
+    d.cfast = I > 1 ? 1 : 0;
+    d.Q = (long long)L * O;
+    d.I = I;
+    d.scale = inverse ? 1.0 / (double)L : 1.0;
+    d.in.kind = d.out.kind = IO_CPLX;
+    d.in.si = d.out.si = 1;
+    d.in.so = d.out.so = I * L;
+    d.in.sk = d.out.sk = I;
+  };
+  fill(p.d, 1);
+  fill(p.d2, L);
+  auto stw = stage_twiddles(dbl, L, rad);
+  p.tables.push_back(stw);
+  p.d.tw = stw->p;
+  auto twl = twiddle_table(dbl, L, 1, 0, L, false);
+  p.tables.push_back(twl);
+  p.d2.tw2 = twl->p;
+  SlabGeom& g = p.sgeom;
+  g.nslab = O;
+  g.tiles = L / k->cs;
+  g.xscale = dbl ? 2 : 1;
+  g.lb = box_rows(L);
+  g.nlb = L / g.lb;
+  g.ntw = k->nst > 1 ? L - rad[0] : 0;
+  const size_t tile = (size_t)k->cs * L * esz;
+  const size_t bstride = (tile + 127) & ~(size_t)127;
+  g.bstride = (int)(bstride / esz);
+  g.err = device_error_word();
+  if (g.nlb > 1 && ((size_t)g.lb * k->cs * esz) % 128 != 0)
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "TMA box offsets would not be 128-byte aligned"};
+  if (((size_t)k->cs * g.xscale * 8) % 16 != 0)
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "TMA rows would not be 16-byte multiples"};
+  // tensor map geometry (encode_map): {L*xscale, L, O}, box {cs*xscale, lb, 1}
+  p.geom.C = k->cs;
+  p.geom.xscale = g.xscale;
+  p.geom.lb = g.lb;
+  p.tI = L;
+  p.tL = L;
+  p.tO = O;
+  const size_t tw_bytes = ((size_t)g.ntw * esz + 127) & ~(size_t)127;
+  p.smem = 128 + tw_bytes + (size_t)kTmaBufs * bstride;
+  p.block = dim3((unsigned)(k->cs * k->P + 32));  // stage threads + producer warp
+  if ((int)p.block.x != k->lb) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "slab kernel block size mismatch"};
+  if (p.smem > max_smem_per_block()) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "slab tiles do not fit"};
+  cuda_check(ensure_smem_attr(p.fn, p.smem), "cudaFuncSetAttribute(slab)");
+  int occ = 0;
+  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p.fn, (int)p.block.x, p.smem),
+             "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (occ < 1) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "slab kernel cannot be resident"};
+  const long long jobs = 2LL * g.tiles * O;
+  long long nb = (long long)sm_count() * occ;
+  if (nb > jobs) nb = jobs;
+  p.grid = dim3((unsigned)nb);
+  // a CTA holds up to kTmaBufs + kSlabClaim claimed jobs: y-jobs trail their
+  // slab's x-jobs by more rounds than the jobs in flight span
+  g.lag = (int)((nb * (kTmaBufs + kSlabClaim) + 2LL * g.tiles - 1) / (2LL * g.tiles)) + 1;
+  p.ctr_bytes = 8 + 4 * (size_t)O;
+  return p;
+}
+
+cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream, void* work) {
   if (p.grid.x == 0) return cudaSuccess;
   cudaError_t e = ensure_smem_attr(p.fn, p.smem);
   if (e != cudaSuccess) return e;
   PassDesc d = p.d;
   d.in.p = in;
   d.out.p = out;
+  if (p.slab) {
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
+      return cudaErrorMisalignedAddress;
+    if (!work || (reinterpret_cast<uintptr_t>(work) & 7)) return cudaErrorInvalidValue;
+    CUtensorMap tout;
+    std::memset(&tout, 0, sizeof(tout));
+    e = encode_map(&tout, out, p);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(work, 0, p.ctr_bytes, stream);
+    if (e != cudaSuccess) return e;
+    PassDesc d2 = p.d2;
+    SlabGeom g = p.sgeom;
+    g.jobs = static_cast<unsigned long long*>(work);
+    g.done = reinterpret_cast<unsigned*>(static_cast<char*>(work) + 8);
+    void* args[] = {&d, &d2, &tout, &g};
+    return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
+  }
   if (p.pipe) {
     if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
       return cudaErrorMisalignedAddress;

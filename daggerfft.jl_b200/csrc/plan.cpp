@@ -79,8 +79,8 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
   for (int a : ax)
     if (S[a] > 0x7fffffffLL) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "axis too long"};
 
-  if (method == DFFT_MIXED && !(is_c2c(transform) && !dbl))
-    throw Error{DFFT_ERROR_INVALID_VALUE, "the mixed form supports ComplexF32 FFT/IFFT only"};
+  if (method == DFFT_MIXED)
+    throw Error{DFFT_ERROR_INVALID_VALUE, "the mixed tensor-core form is not built in this version"};
 
   size_t chirp_bytes = 0;
   auto add = [&](const PassSpec& sp, int src, int dst) {
@@ -115,7 +115,7 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
     std::vector<int> order = ax;
     if (inv) std::reverse(order.begin(), order.end());  // ifft!: dims[3] first
     int src = BUF_IN;
-    for (int a : order) {
+    auto axis_spec = [&](int a) {
       PassSpec s;
       s.dbl = dbl;
       s.L = (int)S[a];
@@ -125,7 +125,34 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
       s.in = io(IO_CPLX, s.I, S[a]);
       s.out = io(IO_CPLX, s.I, S[a]);
       s.fast_io = true;
-      add(s, src, BUF_OUT);
+      return s;
+    };
+    for (size_t i = 0; i < order.size(); ++i) {
+      const int a = order[i];
+      // dims 1 and 2 adjacent in the stage order of an L x L x O array: one
+      // fused 2-D pass per slab (src/fft.jl:735 transforms each slab along
+      // dims (1, 2) before the exchange) when it beats the per-axis passes
+      if (!(flags & DFFT_FLAG_NO_FUSE) && i + 1 < order.size() && a + order[i + 1] == 1 &&
+          S[0] == S[1] && find_slab_kernel(dbl, (int)S[0])) {
+        std::vector<Pass> pair;
+        size_t w = add_axis_passes(pair, axis_spec(a), flags, src, BUF_OUT);
+        w = std::max(w, add_axis_passes(pair, axis_spec(order[i + 1]), flags, BUF_OUT, BUF_OUT));
+        const int v = choose_slab(dbl, (int)S[0], S[2], inv ? 1 : 0, pair, flags);
+        if (v >= 0) {
+          Pass f = make_slab_pass(dbl, (int)S[0], S[2], inv ? 1 : 0, v);
+          f.src = src;
+          f.dst = BUF_OUT;
+          P->work_bytes = std::max(P->work_bytes, f.ctr_bytes);
+          P->passes.push_back(std::move(f));
+        } else {
+          for (Pass& p : pair) P->passes.push_back(std::move(p));
+          chirp_bytes = std::max(chirp_bytes, w);
+        }
+        src = BUF_OUT;
+        ++i;
+        continue;
+      }
+      add(axis_spec(a), src, BUF_OUT);
       src = BUF_OUT;
     }
   } else if (is_rfft(transform)) {
@@ -303,7 +330,7 @@ void execute_plan(const Plan* P, const void* in, void* out, cudaStream_t stream)
   for (const Pass& p : P->passes) {
     if (err != cudaSuccess) break;
     void* bufs[4] = {const_cast<void*>(in), out, P->work, P->chirp};
-    err = launch_pass(p, bufs[p.src], bufs[p.dst], stream);
+    err = launch_pass(p, bufs[p.src], bufs[p.dst], stream, P->work);
   }
   if (cur != P->device) cudaSetDevice(cur);
   cuda_check(err, "kernel launch");

@@ -1,0 +1,300 @@
+// Fused 2-D (dim 1, dim 2) pass over the L x L slabs of an L x L x O array:
+// the Slab decomposition's first stage (a 2-D FFT per slab, src/fft.jl:735,
+// src/fftgpu.jl:541) in ONE sweep of HBM instead of two.
+//
+// Work is a global sequence of jobs.  An x-job transforms CS whole pencils
+// of a slab (one 1-D bulk copy in, stage 1 from the dense tile, the other
+// stages in a swizzled layout in the same buffer, the last stage stored
+// straight to the output with coalesced writes).  A y-job transforms CS
+// columns x L rows of a slab: TMA 3-D boxes of the output, which the slab's
+// x-jobs wrote a moment earlier and which is still in L2, the middle stages
+// in a row-swizzled layout, and a TMA store of the dense result.  The sequence is round-major: round r holds the T = L/CS
+// x-jobs of slab r followed by the T y-jobs of slab r - lag, so a y-job is
+// claimed `lag` rounds after its slab's x-jobs and normally finds them
+// finished; only a few slabs (a few MB) are resident in L2 between the two
+// phases, so every element is read from and written to DRAM once for both
+// axes.
+//
+// Each persistent CTA has CS*P stage threads and one producer warp.  The
+// producer (lane 0) claims runs of consecutive jobs through an atomic
+// counter, works through them in order, waits
+// until a y-job's slab has all its x-tiles, issues the tile loads into
+// kTmaBufs buffers (full barriers), and, when the stage threads hand a buffer
+// back (empty barriers), publishes a finished x-tile in the slab's counter.
+// The stage threads synchronise on named barrier 1 only, so no global atomic
+// or counter wait sits on their path.
+//
+// Progress: x-jobs never wait on other jobs, a CTA works through its claimed
+// jobs in claim order, and a producer publishes its own finished x-tiles
+// before it waits on a slab counter, so the unfinished job with the smallest
+// sequence number can always proceed: the sequence completes whether or not
+// all CTAs are resident.  Every wait (mbarrier, slab counter) is bounded;
+// after a timeout the CTA records DFFT_DEVERR_TMA_TIMEOUT, and every CTA
+// stops claiming jobs once the device error word is set.  The counters (one
+// 64-bit job counter, then one 32-bit counter per slab) are zeroed by the
+// host before each launch.
+#pragma once
+#include "tma_pass.cuh"
+
+namespace dfft {
+
+struct SlabGeom {
+  long long nslab;   // O: slabs in the array (batch included)
+  int tiles;         // T = L / CS tiles per phase per slab
+  int lag;           // rounds between a slab's x-jobs and its y-jobs
+  int xscale;        // TMA x units per complex element (1 float, 2 double)
+  int lb, nlb;       // rows per TMA box, boxes per y tile
+  int ntw;           // stage-twiddle entries staged in shared memory
+  int bstride;       // elements between tile buffers (128-byte multiple)
+  unsigned long long* jobs;  // next job in the sequence
+  unsigned* done;            // x-tiles finished, per slab
+  int* err;
+};
+
+constexpr int kSlabClaim = 1;  // jobs per claim of the slab pass
+
+struct SlabJob {
+  int kind;    // 0 none, 1 x-job, 2 y-job
+  int slab;
+  int tile;
+  int pad;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+// Shared-memory layouts of the tiles between the first and the last stage.
+// Both are XOR permutations inside aligned 128-byte groups (no padding),
+// chosen so that every stage's 32-lane accesses of 8-byte (16-byte) elements
+// fill each 128-byte wavefront: the first stage's radix-R0 writes land
+// R0 elements (x-phase) or R0 rows (y-phase) apart, which the plain layout
+// maps onto the same banks.
+//   x-phase, pencil c, element k:  c*L + xswz(c, k)
+//   y-phase, row k, column c:      yswz(k)*CS + c
+template <int ESZ, int L> __device__ __forceinline__ int xswz(int c, int k) {
+  if constexpr (ESZ == 8 && L == 512) return k ^ (((k >> 4) & 7) | (((k >> 6) & 1) << 3));
+  else if constexpr (ESZ == 8 && L == 256) return k ^ ((k >> 4) & 15);
+  else if constexpr (ESZ == 8 && L == 128) return k ^ (((k >> 4) & 7) | ((c & 1) << 3));
+  else if constexpr (ESZ == 16 && L == 512) return k ^ ((k >> 3) & 7);
+  else if constexpr (ESZ == 16 && L == 256) return k ^ ((k >> 4) & 7);
+  else return k;
+}
+template <int ESZ, int CS, int R0> __device__ __forceinline__ int yswz(int k) {
+  constexpr int slots = 128 / ESZ;                 // elements per 128 bytes
+  constexpr int mask = (slots > CS ? slots / CS : 1) - 1;
+  return k ^ ((k / R0) & mask);
+}
+// Both swizzles are linear over GF(2) in the bits of k (each XORed bit is
+// one bit of k or of c), and a stage's index splits into a per-butterfly
+// base and an offset r * stride with disjoint bits (L and the radices are
+// powers of two), so swz(base | off) = swz(base) ^ swz(off): one swizzle per
+// butterfly and one XOR with a constant per access.
+template <typename V, int L> struct XSwzCol {
+  static_assert((L & (L - 1)) == 0, "bit-split addressing needs a power-of-two length");
+  V* p;  // the pencil's dense start
+  int c;
+  __device__ __forceinline__ int at(int b, int off) const {
+    return xswz<sizeof(V), L>(c, b) ^ xswz<sizeof(V), L>(0, off);
+  }
+  __device__ __forceinline__ V ld(int b, int off) const { return p[at(b, off)]; }
+  __device__ __forceinline__ void st(int b, int off, V v) const { p[at(b, off)] = v; }
+};
+template <typename V, int CS, int R0> struct YSwzCol {
+  static_assert((R0 & (R0 - 1)) == 0, "bit-split addressing needs power-of-two radices");
+  V* p;  // the tile buffer + column
+  __device__ __forceinline__ int at(int b, int off) const {
+    return (yswz<sizeof(V), CS, R0>(b) ^ yswz<sizeof(V), CS, R0>(off)) * CS;
+  }
+  __device__ __forceinline__ V ld(int b, int off) const { return p[at(b, off)]; }
+  __device__ __forceinline__ void st(int b, int off, V v) const { p[at(b, off)] = v; }
+};
+template <int R, int... Rest> struct first_radix { static constexpr int value = R; };
+
+// dx: x-phase descriptor (in -> out, contiguous pencils, FAST_IO global
+// stores); dy: y-phase descriptor (scale / inverse of the second axis).
+// tout: tensor map {L*xscale, L, O} over the output (y-phase loads/stores).
+// Shared memory: [0, 128) full and empty barriers, the stage threads' abort
+// flag (byte 64) and the buffers' job records (byte 80); stage twiddles;
+// kTmaBufs tile buffers.
+// MINB: CTAs per SM the tile buffers allow (register budget per thread).
+template <typename T, int LB, int MINB, int L, int P, int CS, int... Rs>
+__global__ void __launch_bounds__(LB, MINB)
+    slab_xy_pass(const PassDesc dx, const PassDesc dy, const __grid_constant__ CUtensorMap tout,
+                 const SlabGeom g) {
+  typedef typename cvec<T>::type V;
+  constexpr int NC = CS * P;  // stage threads
+  static_assert(NC % 32 == 0 && NC + 32 == LB, "whole warps of stage threads plus one producer warp");
+  extern __shared__ __align__(128) unsigned char smem_slab[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_slab);
+  uint64_t* empty = full + kTmaBufs;
+  int& s_cabort = *reinterpret_cast<int*>(smem_slab + 64);
+  SlabJob* s_job = reinterpret_cast<SlabJob*>(smem_slab + 80);
+  V* stw = reinterpret_cast<V*>(smem_slab + 128);
+  const size_t tw_bytes = ((size_t)g.ntw * sizeof(V) + 127) & ~(size_t)127;
+  V* bufs = reinterpret_cast<V*>(smem_slab + 128 + tw_bytes);
+  const size_t bst = (size_t)g.bstride;
+  const int tid = threadIdx.x;
+  const long long Tt = g.tiles;
+  volatile int* verr = g.err;
+
+  if (tid == 0) {
+    for (int b = 0; b < kTmaBufs; ++b) {
+      mbar_init(&full[b], 1);
+      mbar_init(&empty[b], 1);
+    }
+    mbar_fence_init();
+    s_cabort = 0;
+    const uint32_t a0 = smem_u32(bufs);
+    if ((a0 & 127u) || ((bst * sizeof(V)) & 127u) || (g.nlb > 1 && (((size_t)g.lb * CS * sizeof(V)) & 127u))) {
+      atomicExch(g.err, DFFT_DEVERR_TMA_ALIGN);
+      s_cabort = 1;
+    }
+  }
+  const V* gtw = reinterpret_cast<const V*>(dx.tw);
+  for (int i = tid; i < g.ntw; i += blockDim.x) stw[i] = gtw[i];
+  __syncthreads();
+
+  if (tid >= NC) {
+    if (tid == NC) {
+      // ---------------- producer ----------------
+      const unsigned long long total =
+          (unsigned long long)(g.nslab + g.lag) * 2ull * (unsigned long long)Tt;
+      const uint32_t tile_bytes = (uint32_t)((size_t)CS * L * sizeof(V));
+      int fills[kTmaBufs] = {0, 0, 0};  // arrivals on full[b]
+      int kindb[kTmaBufs] = {0, 0, 0};  // job in buffer b not yet handed back
+      int slabb[kTmaBufs] = {0, 0, 0};
+      bool failed = false;
+      // waits until the stage threads hand buffer b back; publishes an x-tile
+      auto settle = [&](int b) -> bool {
+        if (kindb[b] == 0) return true;
+        if (!mbar_wait_bounded(&empty[b], (uint32_t)((fills[b] - 1) & 1))) return false;
+        if (kindb[b] == 1)  // release: the stage threads' stores, seen through the barrier, first
+          asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(g.done + slabb[b]) : "memory");
+        kindb[b] = 0;
+        return true;
+      };
+      auto wait_slab = [&](int slab) -> bool {
+        const uint64_t t0 = global_ns();
+        for (unsigned i = 0; i < kWaitLimit; ++i) {
+          if (ld_acquire_gpu(g.done + slab) >= (unsigned)Tt) return true;
+          if (*verr != 0) return false;
+          if ((i & 63) == 0 && global_ns() - t0 > kWaitNs) return false;
+          __nanosleep(64);
+        }
+        return false;
+      };
+      // jobs are claimed kSlabClaim at a time (consecutive sequence numbers)
+      unsigned long long next = 0, chunk_end = 0;
+      for (int it = 0;; ++it) {
+        const int b = it % kTmaBufs;
+        if (!settle(b)) { failed = true; break; }
+        SlabJob J{0, 0, 0, 0};
+        while (*verr == 0) {
+          if (next == chunk_end) {
+            next = atomicAdd(g.jobs, (unsigned long long)kSlabClaim);
+            chunk_end = next + kSlabClaim;
+          }
+          const unsigned long long n = next++;
+          if (n >= total) break;
+          const long long r = (long long)(n / (2ull * Tt));
+          const long long i = (long long)(n % (2ull * Tt));
+          if (i < Tt) {
+            if (r >= g.nslab) continue;
+            J = SlabJob{1, (int)r, (int)i, 0};
+          } else {
+            const long long sl = r - g.lag;
+            if (sl < 0 || sl >= g.nslab) continue;
+            J = SlabJob{2, (int)sl, (int)(i - Tt), 0};
+          }
+          break;
+        }
+        if (J.kind == 2 && ld_acquire_gpu(g.done + J.slab) < (unsigned)Tt) {
+          // x-tiles of that slab may sit in this CTA's other buffers:
+          // publish them first
+          bool ok = true;
+          for (int bb = 0; bb < kTmaBufs; ++bb)
+            if (kindb[bb] == 1) ok = settle(bb) && ok;
+          if (!ok || !wait_slab(J.slab)) { failed = true; J.kind = 0; }
+        }
+        s_job[b] = J;
+        ++fills[b];
+        if (J.kind == 0) {
+          mbar_arrive(&full[b]);  // no more work: the stage threads leave
+          break;
+        }
+        V* buf = bufs + b * bst;
+        mbar_expect_tx(&full[b], tile_bytes);
+        if (J.kind == 1) {
+          bulk_load_1d(buf, reinterpret_cast<const V*>(dx.in.p) + ((long long)J.slab * L + (long long)J.tile * CS) * L,
+                       tile_bytes, &full[b]);
+        } else {
+          fence_proxy_async_global();  // x-phase writes (generic proxy) before these async-proxy reads
+          for (int kb = 0; kb < g.nlb; ++kb)
+            tma_load_3d(buf + (size_t)kb * g.lb * CS, &tout, &full[b], J.tile * CS * g.xscale, kb * g.lb, J.slab);
+        }
+        kindb[b] = J.kind;
+        slabb[b] = J.slab;
+      }
+      // publish the x-tiles still held by this CTA
+      for (int bb = 0; bb < kTmaBufs; ++bb)
+        if (!settle(bb)) failed = true;
+      if (failed && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
+      // no bulk copy may still be landing in shared memory when the CTA exits
+      for (int bb = 0; bb < kTmaBufs; ++bb)
+        if (fills[bb] > 0) mbar_wait_bounded(&full[bb], (uint32_t)((fills[bb] - 1) & 1));
+    }
+  } else {
+    // ---------------- stage threads ----------------
+    // both phases have the same length and radices: one stage-twiddle table
+    const StageTw<V> tw{stw};
+    constexpr int R0 = first_radix<Rs...>::value;
+    for (int it = 0;; ++it) {
+      const int b = it % kTmaBufs;
+      if (!mbar_wait_bounded(&full[b], (uint32_t)((it / kTmaBufs) & 1))) s_cabort = 1;
+      stage_sync<NC>();
+      if (s_cabort) break;
+      const SlabJob J = s_job[b];
+      if (J.kind == 0) break;
+      V* buf = bufs + b * bst;
+      if (J.kind == 1) {
+        const int t = tid % P, c = tid / P;
+        const StrideCol<V> dense{buf + (size_t)c * L, 1};
+        const XSwzCol<V, L> sw{buf + (size_t)c * L, c};
+        const long long ob = ((long long)J.slab * L + (long long)J.tile * CS + c) * L;
+        static_stages<T, L, P, true, 2, NC, 1, 1, 0, StrideCol<V>, XSwzCol<V, L>, XSwzCol<V, L>, StageTw<V>,
+                      Rs...>(dx, t, dense, sw, sw, tw, 0, ob, true);
+        fence_proxy_async_global();  // these stores are read by bulk-tensor loads
+      } else {
+        const int c = tid % CS, t = tid / CS;
+        const StrideColC<V, CS> dense{buf + c};
+        const YSwzCol<V, CS, R0> sw{buf + c};
+        static_stages<T, L, P, true, 1, NC, 1, 1, 0, StrideColC<V, CS>, YSwzCol<V, CS, R0>, StrideColC<V, CS>,
+                      StageTw<V>, Rs...>(dy, t, dense, sw, dense, tw, 0, 0, true);
+      }
+      fence_proxy_async_smem();  // the buffer is next read (store) or written (load) by TMA
+      stage_sync<NC>();
+      if (tid == 0) {
+        if (J.kind == 2) {
+          for (int kb = 0; kb < g.nlb; ++kb)
+            tma_store_3d(&tout, buf + (size_t)kb * g.lb * CS, J.tile * CS * g.xscale, kb * g.lb, J.slab);
+          bulk_commit();
+          bulk_wait_read_all();  // the store has read the tile: the buffer goes back
+        }
+        mbar_arrive(&empty[b]);
+      }
+    }
+    if (tid == 0) {
+      bulk_wait_all();
+      if (s_cabort && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace dfft

@@ -158,6 +158,100 @@ Pass tune_pass(const PassSpec& s) {
   return make_pass(t);
 }
 
+int choose_slab(int dbl, int L, long long O, int inverse, const std::vector<Pass>& split,
+                unsigned flags) {
+  std::ostringstream ko;
+  ko << device_tag() << "|slab|" << dbl << "|" << L << "|" << O << "|" << inverse;
+  const std::string key = ko.str();
+  if (!(flags & DFFT_FLAG_NO_WISDOM)) {
+    std::lock_guard<std::mutex> lk(g_w_mu);
+    auto it = g_wisdom.find(key);
+    if (it != g_wisdom.end()) return it->second.variant;
+  }
+  std::vector<Pass> cands;
+  std::vector<int> idx;
+  for (int v = 0; find_slab_kernel(dbl, L, v); ++v) {
+    try {
+      cands.push_back(make_slab_pass(dbl, L, O, inverse, v));
+      idx.push_back(v);
+    } catch (const Error& e) {
+      if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
+    }
+    if (!(flags & DFFT_FLAG_TUNE) && !cands.empty()) return idx[0];
+  }
+  if (cands.empty()) return -1;
+  // time every fused variant and the per-axis pair on scratch arrays
+  const size_t bytes = (size_t)L * L * (size_t)O * (dbl ? 16 : 8);
+  void *in = nullptr, *out = nullptr, *ctr = nullptr;
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto cleanup = [&] {
+    if (in) cudaFree(in);
+    if (out) cudaFree(out);
+    if (ctr) cudaFree(ctr);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st) cudaStreamDestroy(st);
+  };
+  if (cudaMalloc(&in, bytes) != cudaSuccess || cudaMalloc(&out, bytes) != cudaSuccess ||
+      cudaMalloc(&ctr, cands[0].ctr_bytes) != cudaSuccess) {
+    cleanup();
+    cudaGetLastError();
+    return idx[0];
+  }
+  cudaMemset(in, 0, bytes);
+  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const char* ev = std::getenv("DFFT_TUNE_VERBOSE");
+  const bool verbose = ev && ev[0] && ev[0] != '0';
+  auto time_it = [&](const std::vector<const Pass*>& ps) -> float {
+    auto run = [&] {
+      bool ok = true;
+      for (const Pass* p : ps) {
+        void* bufs[2] = {in, out};
+        ok = ok && launch_pass(*p, bufs[p->src == BUF_IN ? 0 : 1], out, st, ctr) == cudaSuccess;
+      }
+      return ok;
+    };
+    for (int i = 0; i < 2; ++i)
+      if (!run()) { cudaGetLastError(); return 1e30f; }
+    const int reps = 5;
+    cudaEventRecord(e0, st);
+    for (int i = 0; i < reps; ++i)
+      if (!run()) { cudaGetLastError(); return 1e30f; }
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) { cudaGetLastError(); return 1e30f; }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms / reps;
+  };
+  int best = -1;
+  float best_ms = 1e30f;
+  if (!split.empty()) {
+    std::vector<const Pass*> ps;
+    for (const Pass& p : split) ps.push_back(&p);
+    best_ms = time_it(ps);
+    if (verbose) std::fprintf(stderr, "dfft tune: slab L=%d O=%lld per-axis passes %.4f ms\n", L, O, best_ms);
+  }
+  for (size_t i = 0; i < cands.size(); ++i) {
+    Pass& p = cands[i];
+    p.src = BUF_IN;
+    p.dst = BUF_OUT;
+    const float ms = time_it({&p});
+    if (verbose)
+      std::fprintf(stderr, "dfft tune: slab L=%d O=%lld variant=%d threads=%u tile=%d lag=%d grid=%u smem=%zu %.4f ms\n",
+                   L, O, idx[i], p.block.x, p.geom.C, p.sgeom.lag, p.grid.x, p.smem, ms);
+    if (ms < best_ms) { best_ms = ms; best = idx[i]; }
+  }
+  cleanup();
+  {
+    std::lock_guard<std::mutex> lk(g_w_mu);
+    g_wisdom[key] = Choice{best, 0, best_ms};
+  }
+  return best;
+}
+
 Pass plan_pass(const PassSpec& s, unsigned flags) {
   if (!(flags & DFFT_FLAG_NO_WISDOM)) {
     int v = 0, C = 0;

@@ -34,6 +34,7 @@ PLAIN, MIXED = 0, 1
 FLAG_DESTROY_INPUT = 1 << 0
 FLAG_TUNE = 1 << 1
 FLAG_NO_WISDOM = 1 << 2
+FLAG_NO_FUSE = 1 << 3
 
 
 class DFFTError(RuntimeError):

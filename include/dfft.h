@@ -71,7 +71,8 @@ typedef enum { DFFT_F32 = 0, DFFT_F64 = 1 } dfft_precision;
 /* decomposition tags (src/fft.jl:13-15) */
 typedef enum { DFFT_PENCIL = 0, DFFT_SLAB = 1 } dfft_decomp;
 
-/* arithmetic form: PLAIN = FP32/FP64 CUDA-core Stockham; MIXED = tensor-core
+/* arithmetic form: PLAIN = FP32/FP64 CUDA-core Stockham; MIXED (reserved: the
+ * tensor-core form is not built in this version, plans return an error) = tensor-core
  * radix-16/32 stages with FP16 hi+lo split products (ComplexF32 only) */
 typedef enum { DFFT_PLAIN = 0, DFFT_MIXED = 1 } dfft_method;
 
@@ -86,7 +87,9 @@ enum {
 enum {
   DFFT_FLAG_DESTROY_INPUT = 1u << 0, /* C2R may use its input as workspace   */
   DFFT_FLAG_TUNE = 1u << 1,          /* time launch candidates at creation   */
-  DFFT_FLAG_NO_WISDOM = 1u << 2      /* ignore the tuning cache              */
+  DFFT_FLAG_NO_WISDOM = 1u << 2,     /* ignore the tuning cache              */
+  DFFT_FLAG_NO_FUSE = 1u << 3        /* one pass per axis: no fused 2-D slab
+                                        pass over dims (1, 2)                */
 };
 
 typedef struct dfft_plan_s* dfft_plan;
