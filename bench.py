@@ -8,9 +8,13 @@ value  : algorithmic GB/s = 2 transforms x 3 axis passes x (read + write of
          the 1 GiB field) = 12.885 GB per step, / step time, summed over ranks.
 e2e    : the same bytes / the time of the public API call sequence with host
          buffers: pinned H2D of the input, fft, ifft, D2H of the result.
-roofline: the slowest axis-pass kernel, timed alone with CUDA events on its
-         stream: 2 x 1 GiB per launch / mean launch time vs the measured
-         HBM copy bandwidth in MEASURED_PEAKS.json.
+roofline: the slowest launch of the step (the fused dims-(1,2) slab pass or
+         an axis pass), timed alone with CUDA events on its stream:
+         algorithmic bytes per launch (2 x 1 GiB per axis it covers) / mean
+         launch time vs the measured HBM copy bandwidth in
+         MEASURED_PEAKS.json.  A fused launch covers two axes with one DRAM
+         sweep, so its fraction can pass 1.0; dram_floor_* gives the rate of
+         that single read + write of the field, and traffic the ncu bytes.
 cpu_baseline: the oracle's restatement of the reference CPU pipeline
          (Blocks(N,N,64) slabs, per-chunk pocketfft with all host threads,
          block redistribution), one forward+inverse of the same 512^3 field.
@@ -172,8 +176,9 @@ def run_reference(args, rank, world):
 
 
 def run_profile(args):
-    """A short, untimed run for ncu: one warm-up and one measured launch of a
-    single axis pass (forward C2C, ComplexF32) on a column-major array."""
+    """A short, untimed run for ncu: two executions of a forward C2C
+    ComplexF32 plan over the --profile dims (one axis pass, or the fused
+    dims-(1,2) slab pass for "12") on a column-major array."""
     import torch
     import dfft
     shape = tuple(int(x) for x in args.shape.split(","))
@@ -291,11 +296,13 @@ def main():
     del A64, F64
     torch.cuda.empty_cache()
 
-    # per-axis kernels timed alone (roofline of the dominant kernel)
-    per_axis = {}
-    for ax in (1, 2, 3):
-        p = dfft.gpu_plan_transform(dfft.FFT(), Ad, (ax,), decomp=decomp, method=args.method,
-                                    flags=flags)
+    # the step's launches timed alone (roofline of the dominant one): the
+    # forward plan is either the fused dims-(1,2) slab pass + the dim-3 pass,
+    # or one pass per axis
+    groups = [(1, 2), (3,)] if pf.launches == 2 else [(1,), (2,), (3,)]
+    per_launch = {}
+    for dims in groups:
+        p = dfft.gpu_plan_transform(dfft.FFT(), Ad, dims, decomp=decomp, method=args.method, flags=flags)
         for _ in range(3):
             p.execute(Ad, Bd, stream)
         a0 = torch.cuda.Event(enable_timing=True)
@@ -306,15 +313,24 @@ def main():
             p.execute(Ad, Bd, stream)
         a1.record(stream)
         torch.cuda.synchronize()
-        per_axis[ax] = a0.elapsed_time(a1) / reps / p.launches
+        per_launch[dims] = (a0.elapsed_time(a1) / reps / p.launches, len(dims) // p.launches)
         del p
-    dom_ax = max(per_axis, key=per_axis.get)
+    dom = max(per_launch, key=lambda k: per_launch[k][0])
+    dom_ms, dom_axes = per_launch[dom]
     peak, peak_kind = measured_peak()
-    achieved = PASS_BYTES / (per_axis[dom_ax] * 1e-3) / 1e9
+    # algorithmic bytes: each axis a launch covers reads and writes the field
+    # once (a fused launch counts its two axes); the DRAM floor of any launch
+    # is one read and one write of the field
+    achieved = dom_axes * PASS_BYTES / (dom_ms * 1e-3) / 1e9
+    dram_floor_gbs = PASS_BYTES / (dom_ms * 1e-3) / 1e9
     traffic = None
     tr = ncu_traffic()
-    if tr and str(dom_ax) in tr.get("axis_pass_bytes", {}):
-        traffic = tr["axis_pass_bytes"][str(dom_ax)]
+    if tr:
+        if len(dom) == 2:
+            traffic = tr.get("slab_pass_bytes")
+        elif str(dom[0]) in tr.get("axis_pass_bytes", {}):
+            traffic = tr["axis_pass_bytes"][str(dom[0])]
+    dom_name = ("fused slab pass dims (1,2)" if len(dom) == 2 else f"axis pass dim {dom[0]}")
 
     # end-to-end through the public API with host buffers
     torch.cuda.synchronize()
@@ -369,8 +385,11 @@ def main():
                        "l2": "inputs (1 GiB) larger than L2 (126 MB); no flush needed"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": traffic, "kernel": f"axis pass dim {dom_ax}",
-                         "per_axis_ms": {str(k): round(v, 4) for k, v in per_axis.items()},
+                         "traffic": traffic, "kernel": dom_name,
+                         "algorithmic_bytes_per_launch": dom_axes * PASS_BYTES,
+                         "dram_floor_gbs": round(dram_floor_gbs, 1),
+                         "dram_floor_frac": round(dram_floor_gbs / peak, 4),
+                         "per_launch_ms": {",".join(map(str, k)): round(v[0], 4) for k, v in per_launch.items()},
                          "step_frac_of_peak": round(value / world / peak, 4)},
             "e2e": {"value": round(e2e, 2), "unit": "GB/s", "ms_per_step": round(e2e_ms, 3),
                     "h2d_bytes_per_step": FIELD_BYTES, "d2h_bytes_per_step": FIELD_BYTES},

@@ -67,6 +67,8 @@ struct SlabKernel {
   int dbl, L, P, nst, radix[4];
   int lb;   // threads per CTA
   int cs;   // pencils / columns per tile
+  int nb;   // tile buffers
+  int dflt; // an untuned plan may pick this variant
   const void* fn;
 };
 // Variant `v` (0-based) for (dbl, L), or null past the last one.
@@ -79,7 +81,8 @@ Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v = 0);
 
 // Fused variant to use for dims (1, 2) of an L x L x O array, or -1 for the
 // per-axis passes `split` (x then y, already planned): wisdom, then timing
-// under DFFT_FLAG_TUNE, else the first variant that builds.
+// under DFFT_FLAG_TUNE, else the first default variant that builds (any
+// variant under DFFT_FLAG_FUSE).
 int choose_slab(int dbl, int L, long long O, int inverse, const std::vector<Pass>& split,
                 unsigned flags);
 

@@ -475,9 +475,6 @@ Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v) {
   const SlabKernel* k = find_slab_kernel(dbl, L, v);
   if (!k) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "no fused slab kernel for this length"};
   if (L % k->cs != 0) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "slab tiling does not divide L"};
-  const StaticPlan* sp = find_static(dbl, L);
-  if (!sp || sp->nst != k->nst || !std::equal(k->radix, k->radix + k->nst, sp->radix))
-    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "fused slab kernel and static plan disagree"};
   if (O < 1 || O >= (1LL << 31)) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "slab count out of range"};
   const int esz = dbl ? 16 : 8;
   const std::vector<int> rad(k->radix, k->radix + k->nst);
@@ -541,7 +538,7 @@ Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v) {
   p.tL = L;
   p.tO = O;
   const size_t tw_bytes = ((size_t)g.ntw * esz + 127) & ~(size_t)127;
-  p.smem = 128 + tw_bytes + (size_t)kTmaBufs * bstride;
+  p.smem = kSlabHeader + tw_bytes + (size_t)k->nb * bstride;
   p.block = dim3((unsigned)(k->cs * k->P + 32));  // stage threads + producer warp
   if ((int)p.block.x != k->lb) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "slab kernel block size mismatch"};
   if (p.smem > max_smem_per_block()) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "slab tiles do not fit"};
@@ -554,9 +551,9 @@ Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v) {
   long long nb = (long long)sm_count() * occ;
   if (nb > jobs) nb = jobs;
   p.grid = dim3((unsigned)nb);
-  // a CTA holds up to kTmaBufs + kSlabClaim claimed jobs: y-jobs trail their
-  // slab's x-jobs by more rounds than the jobs in flight span
-  g.lag = (int)((nb * (kTmaBufs + kSlabClaim) + 2LL * g.tiles - 1) / (2LL * g.tiles)) + 1;
+  // a CTA holds up to (buffers + claim) jobs: y-jobs trail their slab's
+  // x-jobs by more rounds than the jobs in flight span
+  g.lag = (int)((nb * (k->nb + kSlabClaim) + 2LL * g.tiles - 1) / (2LL * g.tiles)) + 1;
   p.ctr_bytes = 8 + 4 * (size_t)O;
   return p;
 }

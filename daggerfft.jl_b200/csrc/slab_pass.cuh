@@ -19,7 +19,7 @@
 // producer (lane 0) claims runs of consecutive jobs through an atomic
 // counter, works through them in order, waits
 // until a y-job's slab has all its x-tiles, issues the tile loads into
-// kTmaBufs buffers (full barriers), and, when the stage threads hand a buffer
+// NB buffers (full barriers), and, when the stage threads hand a buffer
 // back (empty barriers), publishes a finished x-tile in the slab's counter.
 // The stage threads synchronise on named barrier 1 only, so no global atomic
 // or counter wait sits on their path.
@@ -51,7 +51,8 @@ struct SlabGeom {
   int* err;
 };
 
-constexpr int kSlabClaim = 1;  // jobs per claim of the slab pass
+constexpr int kSlabClaim = 1;     // jobs per claim of the slab pass
+constexpr int kSlabHeader = 256;  // shared-memory bytes before the stage twiddles
 
 struct SlabJob {
   int kind;    // 0 none, 1 x-job, 2 y-job
@@ -77,12 +78,13 @@ __device__ __forceinline__ void fence_proxy_async_global() {
 // maps onto the same banks.
 //   x-phase, pencil c, element k:  c*L + xswz(c, k)
 //   y-phase, row k, column c:      yswz(k)*CS + c
-template <int ESZ, int L> __device__ __forceinline__ int xswz(int c, int k) {
-  if constexpr (ESZ == 8 && L == 512) return k ^ (((k >> 4) & 7) | (((k >> 6) & 1) << 3));
-  else if constexpr (ESZ == 8 && L == 256) return k ^ ((k >> 4) & 15);
+template <int ESZ, int L, int R0> __device__ __forceinline__ int xswz(int c, int k) {
+  if constexpr (ESZ == 8 && L == 512 && R0 == 8) return k ^ (((k >> 4) & 7) | (((k >> 6) & 1) << 3));
+  else if constexpr (ESZ == 8 && L == 512 && R0 == 32) return k ^ ((k >> 5) & 15);
+  else if constexpr (ESZ == 8 && L >= 256 && R0 == 16) return k ^ ((k >> 4) & 15);
   else if constexpr (ESZ == 8 && L == 128) return k ^ (((k >> 4) & 7) | ((c & 1) << 3));
-  else if constexpr (ESZ == 16 && L == 512) return k ^ ((k >> 3) & 7);
-  else if constexpr (ESZ == 16 && L == 256) return k ^ ((k >> 4) & 7);
+  else if constexpr (ESZ == 16 && L == 512 && R0 == 8) return k ^ ((k >> 3) & 7);
+  else if constexpr (ESZ == 16 && L >= 256 && R0 == 16) return k ^ ((k >> 4) & 7);
   else return k;
 }
 template <int ESZ, int CS, int R0> __device__ __forceinline__ int yswz(int k) {
@@ -95,12 +97,12 @@ template <int ESZ, int CS, int R0> __device__ __forceinline__ int yswz(int k) {
 // base and an offset r * stride with disjoint bits (L and the radices are
 // powers of two), so swz(base | off) = swz(base) ^ swz(off): one swizzle per
 // butterfly and one XOR with a constant per access.
-template <typename V, int L> struct XSwzCol {
+template <typename V, int L, int R0> struct XSwzCol {
   static_assert((L & (L - 1)) == 0, "bit-split addressing needs a power-of-two length");
   V* p;  // the pencil's dense start
   int c;
   __device__ __forceinline__ int at(int b, int off) const {
-    return xswz<sizeof(V), L>(c, b) ^ xswz<sizeof(V), L>(0, off);
+    return xswz<sizeof(V), L, R0>(c, b) ^ xswz<sizeof(V), L, R0>(0, off);
   }
   __device__ __forceinline__ V ld(int b, int off) const { return p[at(b, off)]; }
   __device__ __forceinline__ void st(int b, int off, V v) const { p[at(b, off)] = v; }
@@ -119,32 +121,33 @@ template <int R, int... Rest> struct first_radix { static constexpr int value = 
 // dx: x-phase descriptor (in -> out, contiguous pencils, FAST_IO global
 // stores); dy: y-phase descriptor (scale / inverse of the second axis).
 // tout: tensor map {L*xscale, L, O} over the output (y-phase loads/stores).
-// Shared memory: [0, 128) full and empty barriers, the stage threads' abort
-// flag (byte 64) and the buffers' job records (byte 80); stage twiddles;
-// kTmaBufs tile buffers.
+// Shared memory: [0, kSlabHeader) full barriers (byte 0), empty barriers
+// (byte 32), the stage threads' abort flag (byte 64) and the buffers' job
+// records (byte 80); stage twiddles; NB tile buffers.
 // MINB: CTAs per SM the tile buffers allow (register budget per thread).
-template <typename T, int LB, int MINB, int L, int P, int CS, int... Rs>
+template <typename T, int LB, int MINB, int NB, int L, int P, int CS, int... Rs>
 __global__ void __launch_bounds__(LB, MINB)
     slab_xy_pass(const PassDesc dx, const PassDesc dy, const __grid_constant__ CUtensorMap tout,
                  const SlabGeom g) {
   typedef typename cvec<T>::type V;
   constexpr int NC = CS * P;  // stage threads
   static_assert(NC % 32 == 0 && NC + 32 == LB, "whole warps of stage threads plus one producer warp");
+  static_assert(NB >= 2 && NB <= 4, "tile buffers");
   extern __shared__ __align__(128) unsigned char smem_slab[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_slab);
-  uint64_t* empty = full + kTmaBufs;
+  uint64_t* empty = reinterpret_cast<uint64_t*>(smem_slab + 32);
   int& s_cabort = *reinterpret_cast<int*>(smem_slab + 64);
   SlabJob* s_job = reinterpret_cast<SlabJob*>(smem_slab + 80);
-  V* stw = reinterpret_cast<V*>(smem_slab + 128);
+  V* stw = reinterpret_cast<V*>(smem_slab + kSlabHeader);
   const size_t tw_bytes = ((size_t)g.ntw * sizeof(V) + 127) & ~(size_t)127;
-  V* bufs = reinterpret_cast<V*>(smem_slab + 128 + tw_bytes);
+  V* bufs = reinterpret_cast<V*>(smem_slab + kSlabHeader + tw_bytes);
   const size_t bst = (size_t)g.bstride;
   const int tid = threadIdx.x;
   const long long Tt = g.tiles;
   volatile int* verr = g.err;
 
   if (tid == 0) {
-    for (int b = 0; b < kTmaBufs; ++b) {
+    for (int b = 0; b < NB; ++b) {
       mbar_init(&full[b], 1);
       mbar_init(&empty[b], 1);
     }
@@ -166,9 +169,9 @@ __global__ void __launch_bounds__(LB, MINB)
       const unsigned long long total =
           (unsigned long long)(g.nslab + g.lag) * 2ull * (unsigned long long)Tt;
       const uint32_t tile_bytes = (uint32_t)((size_t)CS * L * sizeof(V));
-      int fills[kTmaBufs] = {0, 0, 0};  // arrivals on full[b]
-      int kindb[kTmaBufs] = {0, 0, 0};  // job in buffer b not yet handed back
-      int slabb[kTmaBufs] = {0, 0, 0};
+      int fills[NB] = {};  // arrivals on full[b]
+      int kindb[NB] = {};  // job in buffer b not yet handed back
+      int slabb[NB] = {};
       bool failed = false;
       // waits until the stage threads hand buffer b back; publishes an x-tile
       auto settle = [&](int b) -> bool {
@@ -192,7 +195,7 @@ __global__ void __launch_bounds__(LB, MINB)
       // jobs are claimed kSlabClaim at a time (consecutive sequence numbers)
       unsigned long long next = 0, chunk_end = 0;
       for (int it = 0;; ++it) {
-        const int b = it % kTmaBufs;
+        const int b = it % NB;
         if (!settle(b)) { failed = true; break; }
         SlabJob J{0, 0, 0, 0};
         while (*verr == 0) {
@@ -218,7 +221,7 @@ __global__ void __launch_bounds__(LB, MINB)
           // x-tiles of that slab may sit in this CTA's other buffers:
           // publish them first
           bool ok = true;
-          for (int bb = 0; bb < kTmaBufs; ++bb)
+          for (int bb = 0; bb < NB; ++bb)
             if (kindb[bb] == 1) ok = settle(bb) && ok;
           if (!ok || !wait_slab(J.slab)) { failed = true; J.kind = 0; }
         }
@@ -242,11 +245,11 @@ __global__ void __launch_bounds__(LB, MINB)
         slabb[b] = J.slab;
       }
       // publish the x-tiles still held by this CTA
-      for (int bb = 0; bb < kTmaBufs; ++bb)
+      for (int bb = 0; bb < NB; ++bb)
         if (!settle(bb)) failed = true;
       if (failed && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
       // no bulk copy may still be landing in shared memory when the CTA exits
-      for (int bb = 0; bb < kTmaBufs; ++bb)
+      for (int bb = 0; bb < NB; ++bb)
         if (fills[bb] > 0) mbar_wait_bounded(&full[bb], (uint32_t)((fills[bb] - 1) & 1));
     }
   } else {
@@ -255,8 +258,8 @@ __global__ void __launch_bounds__(LB, MINB)
     const StageTw<V> tw{stw};
     constexpr int R0 = first_radix<Rs...>::value;
     for (int it = 0;; ++it) {
-      const int b = it % kTmaBufs;
-      if (!mbar_wait_bounded(&full[b], (uint32_t)((it / kTmaBufs) & 1))) s_cabort = 1;
+      const int b = it % NB;
+      if (!mbar_wait_bounded(&full[b], (uint32_t)((it / NB) & 1))) s_cabort = 1;
       stage_sync<NC>();
       if (s_cabort) break;
       const SlabJob J = s_job[b];
@@ -265,10 +268,10 @@ __global__ void __launch_bounds__(LB, MINB)
       if (J.kind == 1) {
         const int t = tid % P, c = tid / P;
         const StrideCol<V> dense{buf + (size_t)c * L, 1};
-        const XSwzCol<V, L> sw{buf + (size_t)c * L, c};
+        const XSwzCol<V, L, R0> sw{buf + (size_t)c * L, c};
         const long long ob = ((long long)J.slab * L + (long long)J.tile * CS + c) * L;
-        static_stages<T, L, P, true, 2, NC, 1, 1, 0, StrideCol<V>, XSwzCol<V, L>, XSwzCol<V, L>, StageTw<V>,
-                      Rs...>(dx, t, dense, sw, sw, tw, 0, ob, true);
+        static_stages<T, L, P, true, 2, NC, 1, 1, 0, StrideCol<V>, XSwzCol<V, L, R0>, XSwzCol<V, L, R0>,
+                      StageTw<V>, Rs...>(dx, t, dense, sw, sw, tw, 0, ob, true);
         fence_proxy_async_global();  // these stores are read by bulk-tensor loads
       } else {
         const int c = tid % CS, t = tid / CS;

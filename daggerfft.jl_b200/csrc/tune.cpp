@@ -170,14 +170,16 @@ int choose_slab(int dbl, int L, long long O, int inverse, const std::vector<Pass
   }
   std::vector<Pass> cands;
   std::vector<int> idx;
-  for (int v = 0; find_slab_kernel(dbl, L, v); ++v) {
+  const bool tune = (flags & DFFT_FLAG_TUNE) != 0;
+  for (int v = 0; const SlabKernel* k = find_slab_kernel(dbl, L, v); ++v) {
+    if (!tune && !k->dflt && !(flags & DFFT_FLAG_FUSE)) continue;
     try {
       cands.push_back(make_slab_pass(dbl, L, O, inverse, v));
       idx.push_back(v);
     } catch (const Error& e) {
       if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
     }
-    if (!(flags & DFFT_FLAG_TUNE) && !cands.empty()) return idx[0];
+    if (!tune && !cands.empty()) return idx[0];
   }
   if (cands.empty()) return -1;
   // time every fused variant and the per-axis pair on scratch arrays

@@ -5,7 +5,7 @@ compute runs in ``libdfft.so`` (hand-written sm_100a CUDA kernels behind a C
 ABI, see include/dfft.h); this package is the ctypes host layer that mirrors
 the reference's Julia API.
 """
-from ._lib import (FLAG_DESTROY_INPUT, FLAG_NO_FUSE, FLAG_NO_WISDOM, FLAG_TUNE, ArgumentError, DFFTError, LIB_PATH,
+from ._lib import (FLAG_DESTROY_INPUT, FLAG_FUSE, FLAG_NO_FUSE, FLAG_NO_WISDOM, FLAG_TUNE, ArgumentError, DFFTError, LIB_PATH,
                    device_error, lib, wisdom_export, wisdom_forget, wisdom_import, wisdom_size)
 from .api import (Batch, DHT, FFT, FFT_, GPU_PLAN_CACHE, HC2R, IFFT, IFFT_, IRFFT, IRFFT_, R2HC, R2R,
                   R2R_SUPPORTED_KINDS, REDFT00, REDFT01, REDFT10, REDFT11, RFFT, RFFT_, RODFT00,

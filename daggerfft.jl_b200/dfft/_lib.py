@@ -35,6 +35,7 @@ FLAG_DESTROY_INPUT = 1 << 0
 FLAG_TUNE = 1 << 1
 FLAG_NO_WISDOM = 1 << 2
 FLAG_NO_FUSE = 1 << 3
+FLAG_FUSE = 1 << 4
 
 
 class DFFTError(RuntimeError):

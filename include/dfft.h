@@ -88,8 +88,10 @@ enum {
   DFFT_FLAG_DESTROY_INPUT = 1u << 0, /* C2R may use its input as workspace   */
   DFFT_FLAG_TUNE = 1u << 1,          /* time launch candidates at creation   */
   DFFT_FLAG_NO_WISDOM = 1u << 2,     /* ignore the tuning cache              */
-  DFFT_FLAG_NO_FUSE = 1u << 3        /* one pass per axis: no fused 2-D slab
+  DFFT_FLAG_NO_FUSE = 1u << 3,       /* one pass per axis: no fused 2-D slab
                                         pass over dims (1, 2)                */
+  DFFT_FLAG_FUSE = 1u << 4           /* use the fused slab pass wherever a
+                                        kernel exists (no timing)            */
 };
 
 typedef struct dfft_plan_s* dfft_plan;

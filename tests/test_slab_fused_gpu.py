@@ -17,7 +17,8 @@ CASES = [(512, 24, np.complex64), (256, 80, np.complex64), (128, 320, np.complex
          (512, 20, np.complex128), (256, 64, np.complex128)]
 
 
-def _plan(tag, g, dims, flags=0, decomp=None):
+def _plan(tag, g, dims, flags=dfft.FLAG_FUSE, decomp=None):
+    # FLAG_FUSE: the fused kernel wherever one exists, so every length is covered
     return dfft.gpu_plan_transform(tag, g, dims, decomp=decomp, flags=flags)
 
 
@@ -120,3 +121,14 @@ def test_batch_repeats_plan_with_counters():
     torch.cuda.synchronize()
     assert rel(to_np(oa), oracle.fft(a, dims=(1, 2, 3))) <= 1e-5
     assert rel(to_np(ob), oracle.fft(b, dims=(1, 2, 3))) <= 1e-5
+
+
+def test_untuned_default_per_length():
+    # without tuning, 256^2 slabs fuse and 128^2 slabs keep the per-axis
+    # passes (faster at that size); both give the oracle's answer
+    for L, fused in [(256, True), (128, False)]:
+        a = rand((L, L, 16), np.complex64, seed=L)
+        g = to_gpu(a)
+        p = _plan(dfft.FFT(), g, (1, 2), flags=0)
+        assert p.launches == (1 if fused else 2)
+        assert rel(to_np(_run(p, g)), oracle.fft(a, dims=(1, 2))) <= 1e-5
