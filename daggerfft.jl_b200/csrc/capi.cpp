@@ -1,5 +1,8 @@
 // extern "C" entry points of libdfft: argument checks, exception -> status.
 #include <new>
+#include <cstdio>
+#include <cstring>
+#include <string>
 #include "dfft.h"
 #include "dfft_plan.h"
 
@@ -65,6 +68,25 @@ int dfft_plan_launches(dfft_plan plan, int* launches) {
     dfft::Plan* p = impl(plan);
     if (!launches) throw Error{DFFT_ERROR_INVALID_VALUE, "launches is NULL"};
     *launches = (int)p->passes.size();
+  });
+}
+
+int dfft_plan_describe(dfft_plan plan, char* buf, size_t len) {
+  return guarded([&] {
+    dfft::Plan* p = impl(plan);
+    if (!buf || len == 0) throw Error{DFFT_ERROR_INVALID_VALUE, "buf is NULL or len is 0"};
+    std::string out;
+    for (const dfft::Pass& q : p->passes) {
+      const char* kind = q.slab ? "slab-xy" : q.feed ? "strided-feed" : q.pipe ? (q.tma ? "strided-pipe" : "contig-pipe")
+                         : q.is_static ? "direct" : "dynamic";
+      char line[256];
+      std::snprintf(line, sizeof line, "%s L=%d I=%lld O=%lld grid=%u block=%u smem=%zu\n", kind, q.d.L,
+                    q.d.I, q.d.I > 0 ? q.d.Q / q.d.I : 0LL, q.grid.x, q.block.x, q.smem);
+      out += line;
+    }
+    const size_t n = out.size() < len - 1 ? out.size() : len - 1;
+    std::memcpy(buf, out.data(), n);
+    buf[n] = '\0';
   });
 }
 

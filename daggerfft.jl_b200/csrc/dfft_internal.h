@@ -54,6 +54,8 @@ struct Pass {
   // x-phase descriptor, d2 the y-phase one; tensor map as for tma with
   // {tI, tL, tO} = {L, L, O} over the output
   bool slab = false;
+  bool feed = false;     // axis_pass_strided (tensor maps as for tma)
+  StridedGeom fgeom{};
   size_t ctr_bytes = 0;  // job and per-slab counters (in the plan workspace)
   PassDesc d2{};
   SlabGeom sgeom{};
@@ -73,6 +75,8 @@ struct SlabKernel {
 };
 // Variant `v` (0-based) for (dbl, L), or null past the last one.
 const SlabKernel* find_slab_kernel(int dbl, int L, int v = 0);
+// Launch shapes of axis_pass_strided for (dbl, L), same conventions.
+const SlabKernel* find_strided_kernel(int dbl, int L, int v = 0);
 
 // Fused forward or inverse 2-D C2C over dims 1 and 2 of an L x L x O array
 // (scales: 1 forward, 1/L per axis inverse) with launch variant v; throws
@@ -89,7 +93,10 @@ int choose_slab(int dbl, int L, long long O, int inverse, const std::vector<Pass
 // Device error word of the current device (bounded waits that expire set it).
 int* device_error_word();
 
-enum Variant : int { VARIANT_AUTO = 0, VARIANT_DIRECT = 1, VARIANT_PIPE = 2, VARIANT_DYNAMIC = 3 };
+// VARIANT_FEED: strided C2C pass with a producer warp (axis_pass_strided);
+// PassSpec::C then selects the launch shape (index into its kernel table).
+enum Variant : int { VARIANT_AUTO = 0, VARIANT_DIRECT = 1, VARIANT_PIPE = 2, VARIANT_DYNAMIC = 3,
+                     VARIANT_FEED = 4 };
 
 // Pass construction.
 struct PassSpec {

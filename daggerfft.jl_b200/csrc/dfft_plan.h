@@ -31,7 +31,14 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
                  const int32_t* dims, const int32_t* r2r_kinds, int64_t irfft_len, int decomp,
                  int method, unsigned flags);
 
-void execute_plan(const Plan* p, const void* in, void* out, cudaStream_t stream);
+// work / chirp: workspaces supplied by the caller for this execution (null:
+// the plan's own); a plan built with kFlagCallerWorkspace owns none.
+void execute_plan(const Plan* p, const void* in, void* out, cudaStream_t stream, void* work = nullptr,
+                  void* chirp = nullptr);
+
+// Internal plan flag (above the public DFFT_FLAG_* bits): allocate no
+// workspace; every execution brings its own (the serving runtime's arena).
+constexpr unsigned kFlagCallerWorkspace = 1u << 30;
 
 }  // namespace dfft
 

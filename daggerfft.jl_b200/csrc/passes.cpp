@@ -280,7 +280,86 @@ static bool pipe_contig_ok(const PassSpec& s, const StaticPlan* sp, size_t esz) 
   return sp && sp->pipe_c && s.fast_io && !s.epi && s.I == 1 && ((long long)s.L * (long long)esz) % 16 == 0;
 }
 
+static bool feed_ok(const PassSpec& s, size_t esz) {
+  return s.fast_io && !s.epi && s.I > 1 && (s.I * (long long)esz) % 16 == 0 && s.I < (1LL << 31) &&
+         s.O < (1LL << 31) && find_strided_kernel(s.dbl, s.L, 0) != nullptr;
+}
+
+// Strided C2C pass fed by a producer warp (axis_pass_strided); s.C selects
+// the launch shape.
+static Pass make_feed_pass(const PassSpec& s) {
+  const int L = s.L;
+  const int esz = s.dbl ? 16 : 8;
+  if (!feed_ok(s, esz)) throw Error{DFFT_ERROR_INVALID_VALUE, "producer-fed strided variant not available"};
+  const SlabKernel* k = find_strided_kernel(s.dbl, L, s.C < 0 ? 0 : s.C);
+  if (!k) throw Error{DFFT_ERROR_INVALID_VALUE, "no such strided launch shape"};
+  if (s.I < k->cs) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "fewer columns than one tile"};
+  const std::vector<int> rad(k->radix, k->radix + k->nst);
+  Pass p;
+  p.feed = true;
+  p.is_static = true;
+  p.fn = k->fn;
+  PassDesc& d = p.d;
+  d.L = L;
+  d.nst = k->nst;
+  int ns = 1;
+  for (int i = 0; i < d.nst; ++i) {
+    d.radix[i] = rad[i];
+    d.ns[i] = ns;
+    d.tws[i] = L / (ns * rad[i]);
+    ns *= rad[i];
+  }
+  d.P = k->P;
+  d.C = k->cs;
+  d.ld = L;
+  d.inverse = s.inverse;
+  d.cfast = 1;
+  d.Q = s.I * s.O;
+  d.I = s.I;
+  d.scale = s.scale;
+  d.in = s.in;
+  d.out = s.out;
+  for (auto& t : s.keep) p.tables.push_back(t);
+  auto stw = stage_twiddles(s.dbl, L, rad);
+  p.tables.push_back(stw);
+  d.tw = stw->p;
+  StridedGeom& g = p.fgeom;
+  g.xscale = s.dbl ? 2 : 1;
+  g.lb = box_rows(L);
+  g.nlb = L / g.lb;
+  g.tiles_i = (int)((s.I + k->cs - 1) / k->cs);
+  g.ntiles = (long long)g.tiles_i * s.O;
+  g.ntw = k->nst > 1 ? L - rad[0] : 0;
+  const size_t bstride = ((size_t)k->cs * L * esz + 127) & ~(size_t)127;
+  g.bstride = (int)(bstride / esz);
+  g.err = device_error_word();
+  if (g.nlb > 1 && ((size_t)g.lb * k->cs * esz) % 128 != 0)
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "TMA box offsets would not be 128-byte aligned"};
+  if (((size_t)k->cs * g.xscale * 8) % 16 != 0)
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "TMA rows would not be 16-byte multiples"};
+  p.geom.C = k->cs;
+  p.geom.xscale = g.xscale;
+  p.geom.lb = g.lb;
+  p.tI = s.I;
+  p.tL = L;
+  p.tO = s.O;
+  const size_t tw_bytes = ((size_t)g.ntw * esz + 127) & ~(size_t)127;
+  p.smem = kSlabHeader + tw_bytes + (size_t)k->nb * bstride;
+  p.block = dim3((unsigned)k->lb);
+  if (p.smem > max_smem_per_block()) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "strided tiles do not fit"};
+  cuda_check(ensure_smem_attr(p.fn, p.smem), "cudaFuncSetAttribute(strided)");
+  int occ = 0;
+  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p.fn, (int)p.block.x, p.smem),
+             "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (occ < 1) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "strided kernel cannot be resident"};
+  long long nb = (long long)sm_count() * occ;
+  if (nb > g.ntiles) nb = g.ntiles;
+  p.grid = dim3((unsigned)(nb > 0 ? nb : 1));
+  return p;
+}
+
 Pass make_pass(const PassSpec& s) {
+  if (s.variant == VARIANT_FEED) return make_feed_pass(s);
   Pass p;
   PassDesc& d = p.d;
   const int L = s.L;
@@ -291,6 +370,18 @@ Pass make_pass(const PassSpec& s) {
   if (sp && sp->P > sp->lb) sp = nullptr;
   int variant = s.variant;
   if (variant == VARIANT_AUTO) {
+    // strided axes: the producer-fed kernel unless rows lie 1 MiB or more
+    // apart (each tile then touches L pages, and the narrower tile rows of
+    // that kernel pay the address translation twice as often)
+    if (feed_ok(s, esz) && s.I * (long long)esz < (1LL << 20)) {
+      PassSpec t = s;
+      t.variant = VARIANT_FEED;
+      t.C = 0;
+      try {
+        return make_pass(t);
+      } catch (const Error&) {
+      }
+    }
     if (pipe_strided_ok(s, sp, esz) || pipe_contig_ok(s, sp, esz)) {
       PassSpec t = s;
       t.variant = VARIANT_PIPE;
@@ -565,6 +656,20 @@ cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream,
   PassDesc d = p.d;
   d.in.p = in;
   d.out.p = out;
+  if (p.feed) {
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
+      return cudaErrorMisalignedAddress;
+    CUtensorMap tin, tout;
+    std::memset(&tin, 0, sizeof(tin));
+    std::memset(&tout, 0, sizeof(tout));
+    e = encode_map(&tin, in, p);
+    if (e != cudaSuccess) return e;
+    e = encode_map(&tout, out, p);
+    if (e != cudaSuccess) return e;
+    StridedGeom g = p.fgeom;
+    void* args[] = {&d, &tin, &tout, &g};
+    return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
+  }
   if (p.slab) {
     if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
       return cudaErrorMisalignedAddress;

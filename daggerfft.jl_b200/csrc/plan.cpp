@@ -297,9 +297,9 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
     }
   }
   P->chirp_bytes = chirp_bytes;
-  if (chirp_bytes) cuda_check(cudaMalloc(&P->chirp, chirp_bytes), "cudaMalloc(bluestein scratch)");
-  if (P->work_bytes) {
-    cuda_check(cudaMalloc(&P->work, P->work_bytes), "cudaMalloc(workspace)");
+  if (!(flags & kFlagCallerWorkspace)) {
+    if (chirp_bytes) cuda_check(cudaMalloc(&P->chirp, chirp_bytes), "cudaMalloc(bluestein scratch)");
+    if (P->work_bytes) cuda_check(cudaMalloc(&P->work, P->work_bytes), "cudaMalloc(workspace)");
   }
   return P.release();
 }
@@ -318,8 +318,12 @@ Plan::~Plan() {
 size_t Plan::in_bytes() const { return (size_t)(in_shape[0] * in_shape[1] * in_shape[2]) * in_elem; }
 size_t Plan::out_bytes() const { return (size_t)(out_shape[0] * out_shape[1] * out_shape[2]) * out_elem; }
 
-void execute_plan(const Plan* P, const void* in, void* out, cudaStream_t stream) {
+void execute_plan(const Plan* P, const void* in, void* out, cudaStream_t stream, void* work, void* chirp) {
   if (!in || !out) throw Error{DFFT_ERROR_INVALID_VALUE, "in/out is NULL"};
+  if (!work) work = P->work;
+  if (!chirp) chirp = P->chirp;
+  if ((P->work_bytes && !work) || (P->chirp_bytes && !chirp))
+    throw Error{DFFT_ERROR_INVALID_VALUE, "plan has no workspace and none was supplied"};
   int cur = -1;
   cuda_check(cudaGetDevice(&cur), "cudaGetDevice");
   if (cur != P->device) cuda_check(cudaSetDevice(P->device), "cudaSetDevice");
@@ -329,8 +333,8 @@ void execute_plan(const Plan* P, const void* in, void* out, cudaStream_t stream)
   }
   for (const Pass& p : P->passes) {
     if (err != cudaSuccess) break;
-    void* bufs[4] = {const_cast<void*>(in), out, P->work, P->chirp};
-    err = launch_pass(p, bufs[p.src], bufs[p.dst], stream, P->work);
+    void* bufs[4] = {const_cast<void*>(in), out, work, chirp};
+    err = launch_pass(p, bufs[p.src], bufs[p.dst], stream, work);
   }
   if (cur != P->device) cudaSetDevice(cur);
   cuda_check(err, "kernel launch");

@@ -6,9 +6,9 @@
 // request's staging memory fits the HBM budget -- an arena carved once at
 // creation, so admission never calls cudaMalloc.  Each admitted request
 // runs on its own stream: optional host->device copy into the arena, the
-// transform (plans, twiddles and workspaces stay resident in a plan cache;
-// workspace-free plans are shared by concurrent requests, the others get
-// one instance per concurrently running request of a shape), an
+// transform (one resident plan per shape, shared by concurrent requests;
+// each request's workspace -- C2R or Bluestein scratch, fused-pass
+// counters -- comes from the arena beside its staging memory), an
 // optional device->host copy, and a host callback that timestamps the
 // completion and wakes the dispatcher, which frees the slot and the arena
 // memory and admits the next requests.  Work of different requests overlaps
@@ -116,8 +116,9 @@ struct Req {
   int state = 0;             // 0 queued, 1 running, 2 done, 3 cancelled, 4 failed
   int status = 0;
   int slot = -1;
-  size_t off_in = 0, off_out = 0;
-  bool has_in = false, has_out = false;
+  size_t off_in = 0, off_out = 0, off_work = 0;
+  bool has_in = false, has_out = false, has_work = false;
+  size_t work_bytes = 0, chirp_bytes = 0;  // the plan's workspaces, from the arena
   Plan* plan = nullptr;
 };
 
@@ -149,8 +150,7 @@ struct Server {
   std::unordered_map<uint64_t, Req*> reqs;
   std::deque<uint64_t> completed;   // finished, not yet polled
   std::vector<double> lat_ms;
-  std::multimap<PlanKey, Plan*> idle_plans;   // exclusive plans not in use
-  std::map<PlanKey, Plan*> shared_plans;      // workspace-free plans
+  std::map<PlanKey, Plan*> shared_plans;      // one resident plan per shape
   std::vector<Plan*> all_plans;
   uint64_t next_id = 1;
   bool stop = false;
@@ -172,30 +172,21 @@ static void CUDART_CB on_done(void* p) {
   s->srv->cv.notify_all();
 }
 
-// A plan without a workspace only reads its tables while it runs, so one
-// instance serves every concurrent request of its shape; a plan with a
-// workspace (multi-dim irfft, Bluestein) is used by one request at a time.
-static bool shareable(const Plan* p) { return p->work_bytes == 0 && p->chirp_bytes == 0; }
-
+// Server plans own no workspace (kFlagCallerWorkspace): while it runs a
+// plan only reads its tables, and each request brings its workspace (C2R
+// scratch, Bluestein scratch, fused-pass counters) from the arena, so one
+// resident instance serves every concurrent request of its shape.
 static Plan* get_plan(Server* S, const PlanKey& k, const dfft_request& r) {
   auto sh = S->shared_plans.find(k);
   if (sh != S->shared_plans.end()) return sh->second;
-  auto it = S->idle_plans.find(k);
-  if (it != S->idle_plans.end()) {
-    Plan* p = it->second;
-    S->idle_plans.erase(it);
-    return p;
-  }
-  Plan* p = build_plan(r.ndim, r.shape, r.precision, r.transform, r.ndims, r.dims, r.r2r_kinds,
-                       r.irfft_len, r.decomp, DFFT_PLAIN, S->flags & DFFT_FLAG_TUNE);
+  Plan* p = build_plan(r.ndim, r.shape, r.precision, r.transform, r.ndims, r.dims, r.r2r_kinds, r.irfft_len,
+                       r.decomp, DFFT_PLAIN, (S->flags & DFFT_FLAG_TUNE) | kFlagCallerWorkspace);
   S->all_plans.push_back(p);
-  if (shareable(p)) S->shared_plans[k] = p;
+  S->shared_plans[k] = p;
   return p;
 }
 
-static void put_plan(Server* S, const PlanKey& k, Plan* p) {
-  if (!shareable(p)) S->idle_plans.emplace(k, p);
-}
+static size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // Admit queued requests in order while a slot and arena memory are free.
 static void admit(Server* S, std::unique_lock<std::mutex>& lk) {
@@ -225,11 +216,23 @@ static void admit(Server* S, std::unique_lock<std::mutex>& lk) {
       }
       gout = true;
     }
+    size_t owork = 0;
+    bool gwork = false;
+    if (q->work_bytes + q->chirp_bytes) {
+      if (!S->arena.alloc(round256(q->work_bytes) + q->chirp_bytes, &owork)) {
+        if (gin) S->arena.release(oin);
+        if (gout) S->arena.release(oout);
+        return;
+      }
+      gwork = true;
+    }
     S->queue.pop_front();
     q->off_in = oin;
     q->off_out = oout;
+    q->off_work = owork;
     q->has_in = gin;
     q->has_out = gout;
+    q->has_work = gwork;
     q->slot = free_slot;
     q->state = 1;
     q->t_admit = Clock::now();
@@ -256,7 +259,9 @@ static void admit(Server* S, std::unique_lock<std::mutex>& lk) {
         if (gin)
           cuda_check(cudaMemcpyAsync((void*)din, q->r.in, q->in_bytes, cudaMemcpyHostToDevice, sl.stream),
                      "cudaMemcpyAsync(H2D)");
-        execute_plan(q->plan, din, dout, sl.stream);
+        char* w = gwork ? S->arena_base + owork : nullptr;
+        execute_plan(q->plan, din, dout, sl.stream, q->work_bytes ? w : nullptr,
+                     q->chirp_bytes ? w + round256(q->work_bytes) : nullptr);
         if (q->r.out_location == DFFT_MEM_HOST)
           cuda_check(cudaMemcpyAsync(q->r.out, dout, q->out_bytes, cudaMemcpyDeviceToHost, sl.stream),
                      "cudaMemcpyAsync(D2H)");
@@ -297,7 +302,10 @@ static void retire(Server* S) {
       S->arena.release(q->off_out);
       q->has_out = false;
     }
-    if (q->plan) put_plan(S, q->key, q->plan);
+    if (q->has_work) {
+      S->arena.release(q->off_work);
+      q->has_work = false;
+    }
     q->plan = nullptr;
     if (q->state == 2) {
       S->n_done++;
@@ -424,9 +432,12 @@ int dfft_server_submit(dfft_server server, const dfft_request* req, uint64_t* id
     dfft::Plan* p = dfft::get_plan(S, k, *req);
     q->in_bytes = p->in_bytes();
     q->out_bytes = p->out_bytes();
-    dfft::put_plan(S, k, p);
-    q->stage_bytes = (req->in_location == DFFT_MEM_HOST ? ((q->in_bytes + 255) & ~(size_t)255) : 0) +
-                     (req->out_location != DFFT_MEM_DEVICE ? ((q->out_bytes + 255) & ~(size_t)255) : 0);
+    q->work_bytes = p->work_bytes;
+    q->chirp_bytes = p->chirp_bytes;
+    q->stage_bytes = (req->in_location == DFFT_MEM_HOST ? dfft::round256(q->in_bytes) : 0) +
+                     (req->out_location != DFFT_MEM_DEVICE ? dfft::round256(q->out_bytes) : 0) +
+                     (q->work_bytes + q->chirp_bytes ? dfft::round256(dfft::round256(q->work_bytes) + q->chirp_bytes)
+                                                      : 0);
     if (q->stage_bytes > S->arena.size()) {
       S->n_rejected++;
       throw Error{DFFT_ERROR_OUT_OF_MEMORY, "request needs " + std::to_string(q->stage_bytes) +

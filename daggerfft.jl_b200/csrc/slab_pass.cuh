@@ -301,3 +301,134 @@ __global__ void __launch_bounds__(LB, MINB)
 }
 
 }  // namespace dfft
+
+namespace dfft {
+
+// ---------------------------------------------------------------------------
+// Strided-axis pass with a producer warp (the y-phase machinery of the slab
+// pass without the slab dependency): tile t of the tensor {I*xscale, L, O}
+// is CS columns x L rows (x = (t % tiles_i)*CS, z = t / tiles_i), loaded
+// and stored by TMA boxes {CS*xscale, lb, 1}; CTA b takes tiles b, b+grid, ...
+// The producer (lane 0 of the last warp) fills NB buffers as the stage
+// threads hand them back; the stage threads run the stages in the
+// row-swizzled layout with the stage twiddles in shared memory and sync on
+// named barrier 1.  Bounded waits as in the slab pass.
+// ---------------------------------------------------------------------------
+
+struct StridedGeom {
+  long long ntiles;  // tiles_i * O
+  int tiles_i;       // tiles along I
+  int xscale, lb, nlb;
+  int ntw, bstride;
+  int* err;
+};
+
+template <typename T, int LB, int MINB, int NB, int L, int P, int CS, int... Rs>
+__global__ void __launch_bounds__(LB, MINB)
+    axis_pass_strided(const PassDesc d, const __grid_constant__ CUtensorMap tin,
+                      const __grid_constant__ CUtensorMap tout, const StridedGeom g) {
+  typedef typename cvec<T>::type V;
+  constexpr int NC = CS * P;
+  static_assert(NC % 32 == 0 && NC + 32 == LB, "whole warps of stage threads plus one producer warp");
+  static_assert(NB >= 2 && NB <= 4, "tile buffers");
+  constexpr int R0 = first_radix<Rs...>::value;
+  extern __shared__ __align__(128) unsigned char smem_str[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_str);
+  uint64_t* empty = reinterpret_cast<uint64_t*>(smem_str + 32);
+  int& s_cabort = *reinterpret_cast<int*>(smem_str + 64);
+  long long* s_tile = reinterpret_cast<long long*>(smem_str + 80);  // NB entries
+  V* stw = reinterpret_cast<V*>(smem_str + kSlabHeader);
+  const size_t tw_bytes = ((size_t)g.ntw * sizeof(V) + 127) & ~(size_t)127;
+  V* bufs = reinterpret_cast<V*>(smem_str + kSlabHeader + tw_bytes);
+  const size_t bst = (size_t)g.bstride;
+  const int tid = threadIdx.x;
+  volatile int* verr = g.err;
+
+  if (tid == 0) {
+    for (int b = 0; b < NB; ++b) {
+      mbar_init(&full[b], 1);
+      mbar_init(&empty[b], 1);
+    }
+    mbar_fence_init();
+    s_cabort = 0;
+    const uint32_t a0 = smem_u32(bufs);
+    if ((a0 & 127u) || ((bst * sizeof(V)) & 127u) || (g.nlb > 1 && (((size_t)g.lb * CS * sizeof(V)) & 127u))) {
+      atomicExch(g.err, DFFT_DEVERR_TMA_ALIGN);
+      s_cabort = 1;
+    }
+  }
+  const V* gtw = reinterpret_cast<const V*>(d.tw);
+  for (int i = tid; i < g.ntw; i += blockDim.x) stw[i] = gtw[i];
+  __syncthreads();
+
+  if (tid >= NC) {
+    if (tid == NC) {
+      // ---------------- producer ----------------
+      const uint32_t tile_bytes = (uint32_t)((size_t)CS * L * sizeof(V));
+      int fills[NB] = {};
+      bool failed = false;
+      long long tile = blockIdx.x;
+      for (int it = 0;; ++it) {
+        const int b = it % NB;
+        // the buffer's previous tile must be handed back first
+        if (fills[b] > 0 && !mbar_wait_bounded(&empty[b], (uint32_t)((fills[b] - 1) & 1))) {
+          failed = true;
+          break;
+        }
+        const bool more = tile < g.ntiles && *verr == 0 && !s_cabort;
+        s_tile[b] = more ? tile : -1;
+        ++fills[b];
+        if (!more) {
+          mbar_arrive(&full[b]);  // no more tiles: the stage threads leave
+          break;
+        }
+        const int ti = (int)(tile % g.tiles_i);
+        const int o = (int)(tile / g.tiles_i);
+        V* buf = bufs + b * bst;
+        mbar_expect_tx(&full[b], tile_bytes);
+        for (int kb = 0; kb < g.nlb; ++kb)
+          tma_load_3d(buf + (size_t)kb * g.lb * CS, &tin, &full[b], ti * CS * g.xscale, kb * g.lb, o);
+        tile += gridDim.x;
+      }
+      if (failed && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
+      // no bulk copy may still be landing in shared memory when the CTA exits
+      for (int bb = 0; bb < NB; ++bb)
+        if (fills[bb] > 0) mbar_wait_bounded(&full[bb], (uint32_t)((fills[bb] - 1) & 1));
+    }
+  } else {
+    // ---------------- stage threads ----------------
+    const StageTw<V> tw{stw};
+    const int c = tid % CS, t = tid / CS;
+    for (int it = 0;; ++it) {
+      const int b = it % NB;
+      if (!mbar_wait_bounded(&full[b], (uint32_t)((it / NB) & 1))) s_cabort = 1;
+      stage_sync<NC>();
+      if (s_cabort) break;
+      const long long tile = s_tile[b];
+      if (tile < 0) break;
+      V* buf = bufs + b * bst;
+      const StrideColC<V, CS> dense{buf + c};
+      const YSwzCol<V, CS, R0> sw{buf + c};
+      static_stages<T, L, P, true, 1, NC, 1, 1, 0, StrideColC<V, CS>, YSwzCol<V, CS, R0>, StrideColC<V, CS>,
+                    StageTw<V>, Rs...>(d, t, dense, sw, dense, tw, 0, 0, true);
+      fence_proxy_async_smem();
+      stage_sync<NC>();
+      if (tid == 0) {
+        const int ti = (int)(tile % g.tiles_i);
+        const int o = (int)(tile / g.tiles_i);
+        for (int kb = 0; kb < g.nlb; ++kb)
+          tma_store_3d(&tout, buf + (size_t)kb * g.lb * CS, ti * CS * g.xscale, kb * g.lb, o);
+        bulk_commit();
+        bulk_wait_read_all();  // the store has read the tile: the buffer goes back
+        mbar_arrive(&empty[b]);
+      }
+    }
+    if (tid == 0) {
+      bulk_wait_all();
+      if (s_cabort && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace dfft

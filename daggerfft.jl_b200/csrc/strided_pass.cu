@@ -1,0 +1,58 @@
+// Instantiations of the producer-warp strided axis pass (axis_pass_strided)
+// and its launch shapes, fastest first (B200, 512^3 / 256^3 / 128^3 arrays).
+// threads = CS*P stage threads + one producer warp; MINB = CTAs per SM that
+// NB tile buffers of CS*L elements leave room for.
+#include "dfft_internal.h"
+
+namespace dfft {
+
+#define DFFT_STRIDED_INST(T, LB, MINB, NB, L, P, CS, ...)                                              \
+  template __global__ void axis_pass_strided<T, LB, MINB, NB, L, P, CS, __VA_ARGS__>(                \
+      const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap,       \
+      const StridedGeom);
+#define K(T, LB, MINB, NB, L, P, CS, ...) (const void*)&axis_pass_strided<T, LB, MINB, NB, L, P, CS, __VA_ARGS__>
+
+// ComplexF32, L = 512 (8 x 8 x 8)
+DFFT_STRIDED_INST(float, 288, 3, 2, 512, 32, 8, 8, 8, 8)
+DFFT_STRIDED_INST(float, 288, 2, 3, 512, 32, 8, 8, 8, 8)
+DFFT_STRIDED_INST(float, 160, 6, 2, 512, 32, 4, 8, 8, 8)
+DFFT_STRIDED_INST(float, 544, 1, 2, 512, 32, 16, 8, 8, 8)
+// ComplexF32, L = 256 (16 x 16) and 128 (16 x 8)
+DFFT_STRIDED_INST(float, 288, 3, 2, 256, 16, 16, 16, 16)
+DFFT_STRIDED_INST(float, 288, 2, 3, 256, 16, 16, 16, 16)
+DFFT_STRIDED_INST(float, 160, 6, 2, 256, 16, 8, 16, 16)
+DFFT_STRIDED_INST(float, 160, 6, 2, 128, 8, 16, 16, 8)
+DFFT_STRIDED_INST(float, 160, 4, 3, 128, 8, 16, 16, 8)
+// ComplexF64, L = 512 and 256
+DFFT_STRIDED_INST(double, 288, 3, 2, 512, 64, 4, 8, 8, 8)
+DFFT_STRIDED_INST(double, 160, 4, 2, 512, 32, 4, 8, 8, 8)
+DFFT_STRIDED_INST(double, 160, 3, 2, 256, 16, 8, 16, 16)
+DFFT_STRIDED_INST(double, 96, 5, 2, 256, 16, 4, 16, 16)
+
+static const SlabKernel kStridedKernels[] = {
+    // dbl, L, P, nst, radices, threads, CS, NB, dflt, kernel
+    {0, 512, 32, 3, {8, 8, 8}, 288, 8, 3, 1, K(float, 288, 2, 3, 512, 32, 8, 8, 8, 8)},
+    {0, 512, 32, 3, {8, 8, 8}, 288, 8, 2, 1, K(float, 288, 3, 2, 512, 32, 8, 8, 8, 8)},
+    {0, 512, 32, 3, {8, 8, 8}, 160, 4, 2, 1, K(float, 160, 6, 2, 512, 32, 4, 8, 8, 8)},
+    {0, 512, 32, 3, {8, 8, 8}, 544, 16, 2, 1, K(float, 544, 1, 2, 512, 32, 16, 8, 8, 8)},
+    {0, 256, 16, 2, {16, 16}, 288, 16, 2, 1, K(float, 288, 3, 2, 256, 16, 16, 16, 16)},
+    {0, 256, 16, 2, {16, 16}, 288, 16, 3, 1, K(float, 288, 2, 3, 256, 16, 16, 16, 16)},
+    {0, 256, 16, 2, {16, 16}, 160, 8, 2, 1, K(float, 160, 6, 2, 256, 16, 8, 16, 16)},
+    {0, 128, 8, 2, {16, 8}, 160, 16, 2, 1, K(float, 160, 6, 2, 128, 8, 16, 16, 8)},
+    {0, 128, 8, 2, {16, 8}, 160, 16, 3, 1, K(float, 160, 4, 3, 128, 8, 16, 16, 8)},
+    {1, 512, 64, 3, {8, 8, 8}, 288, 4, 2, 1, K(double, 288, 3, 2, 512, 64, 4, 8, 8, 8)},
+    {1, 512, 32, 3, {8, 8, 8}, 160, 4, 2, 1, K(double, 160, 4, 2, 512, 32, 4, 8, 8, 8)},
+    {1, 256, 16, 2, {16, 16}, 160, 8, 2, 1, K(double, 160, 3, 2, 256, 16, 8, 16, 16)},
+    {1, 256, 16, 2, {16, 16}, 96, 4, 2, 1, K(double, 96, 5, 2, 256, 16, 4, 16, 16)},
+};
+
+#undef K
+
+const SlabKernel* find_strided_kernel(int dbl, int L, int v) {
+  int i = 0;
+  for (const SlabKernel& k : kStridedKernels)
+    if (k.dbl == dbl && k.L == L && i++ == v) return &k;
+  return nullptr;
+}
+
+}  // namespace dfft

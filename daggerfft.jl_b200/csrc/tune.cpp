@@ -93,6 +93,17 @@ Pass tune_pass(const PassSpec& s) {
         cands.push_back({v, C});
     }
   }
+  // producer-fed strided kernels: one candidate per launch shape
+  for (int i = 0; find_strided_kernel(s.dbl, s.L, i); ++i) {
+    PassSpec t = s;
+    t.variant = VARIANT_FEED;
+    t.C = i;
+    try {
+      make_pass(t);
+      cands.push_back({VARIANT_FEED, i});
+    } catch (const Error&) {
+    }
+  }
   if (cands.empty()) return make_pass(s);
   const size_t ib = side_bytes(s, s.in, false), ob = side_bytes(s, s.out, true);
   void *in = nullptr, *out = nullptr;
@@ -129,7 +140,7 @@ Pass tune_pass(const PassSpec& s) {
     } catch (const Error&) {
       continue;
     }
-    if ((int)p.d.C != vc.second) continue;  // clamped to another candidate
+    if (vc.first != VARIANT_FEED && (int)p.d.C != vc.second) continue;  // clamped to another candidate
     bool ok = true;
     for (int i = 0; i < 2 && ok; ++i) ok = launch_pass(p, in, out, st) == cudaSuccess;
     if (!ok) { cudaGetLastError(); continue; }

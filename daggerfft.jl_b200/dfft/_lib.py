@@ -78,6 +78,8 @@ def lib():
     L.dfft_plan_workspace_bytes.restype = c_int
     L.dfft_plan_launches.argtypes = [c_void_p, ctypes.POINTER(c_int)]
     L.dfft_plan_launches.restype = c_int
+    L.dfft_plan_describe.argtypes = [c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    L.dfft_plan_describe.restype = c_int
     L.dfft_execute.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
     L.dfft_execute.restype = c_int
     L.dfft_plan_destroy.argtypes = [c_void_p]

@@ -218,6 +218,13 @@ class Plan:
         check(L.dfft_plan_workspace_bytes(h, ctypes.byref(wb)))
         self.workspace_bytes = wb.value
 
+    def describe(self) -> str:
+        """One line per kernel launch (kernel kind, length, columns, launch
+        shape): ``dfft_plan_describe``."""
+        buf = ctypes.create_string_buffer(8192)
+        check(self._L.dfft_plan_describe(self._h, buf, ctypes.c_size_t(len(buf))))
+        return buf.value.decode()
+
     def execute(self, inp: torch.Tensor, out: torch.Tensor, stream=None):
         if stream is None:
             stream = torch.cuda.current_stream(inp.device)

@@ -124,6 +124,11 @@ DFFT_API int dfft_plan_workspace_bytes(dfft_plan plan, size_t* bytes);
 /* Number of kernel launches one dfft_execute makes. */
 DFFT_API int dfft_plan_launches(dfft_plan plan, int* launches);
 
+/* One line per kernel launch of the plan ("<kernel> L=.. I=.. O=.. grid=..
+ * block=.. smem=.."), NUL-terminated and truncated to len-1 characters
+ * (the analogue of fftw_sprint_plan; for logs and tests). */
+DFFT_API int dfft_plan_describe(dfft_plan plan, char* buf, size_t len);
+
 /*
  * Execute: out = T(in).  Replaces apply_fft! / apply_gpu_fft!
  * (`mul!(out, plan, in)`, src/fft.jl:168-174, src/fftgpu.jl:118-124) and
@@ -181,8 +186,9 @@ DFFT_API int dfft_batch_destroy(dfft_batch batch);
  * streams.  Requests are admitted in arrival order while a slot is free and
  * their staging memory (host input copied in, host or server-held output)
  * fits the arena; admitted requests run concurrently on their own streams
- * and new ones join as slots and memory free up.  Plans, twiddles and
- * workspaces stay resident per shape.  Every request must be released
+ * and new ones join as slots and memory free up.  Plans and twiddles stay
+ * resident per shape (one plan serves concurrent requests); a request's
+ * plan workspace, if any, is taken from the arena with its staging memory.  Every request must be released
  * (dfft_server_release) after it finishes.
  */
 enum { DFFT_MEM_DEVICE = 0, DFFT_MEM_HOST = 1, DFFT_MEM_SERVER = 2 };

@@ -89,6 +89,46 @@ def test_alone_equals_in_the_mix():
         assert rel(to_np(y), ref) <= tol
 
 
+def test_workspace_plans_shared_under_concurrency():
+    # plans whose executions need scratch memory -- fused slab-pass counters
+    # (256 x 256 x 16 ComplexF32), Bluestein scratch (prime edges 17 and 31),
+    # C2R scratch (irfft over three dims) -- run 8 at a time from one
+    # resident plan each, every request with its own workspace from the arena
+    a1 = rand((256, 256, 16), np.complex64, seed=1)
+    a2 = rand((17, 31, 8), np.complex64, seed=2)
+    a3 = oracle.rfft(rand((32, 24, 16), np.float32, seed=3)).astype(np.complex64)
+    srv = dfft.Server(1 << 30, slots=8)
+    jobs = []
+    for t, a, n in [(dfft.FFT(), a1, None), (dfft.IFFT(), a2, None), (dfft.IRFFT(), a3, 32)]:
+        g = to_gpu(a)
+        shp, dt = _out_meta(t, a, n)
+        for _ in range(8):
+            o = dfft.empty_like_layout(shp, dt, g)
+            jobs.append((t, a, n, o, srv.submit(t, g, dims=(1, 2, 3), n=n, out=o)))
+    for *_, rid in jobs:
+        assert srv.wait(rid, 20000) == 0
+        srv.release(rid)
+    torch.cuda.synchronize()
+    st = srv.stats()
+    assert st["completed"] == len(jobs) and st["failed"] == 0
+    assert st["resident_plans"] == 3
+    assert dfft.device_error() == 0
+    first = {}
+    for t, a, n, o, _ in jobs:
+        if isinstance(t, dfft.FFT):
+            ref = oracle.fft(a, dims=(1, 2, 3))
+        elif isinstance(t, dfft.IFFT):
+            ref = oracle.ifft(a, dims=(1, 2, 3))
+        else:
+            ref = oracle.irfft(a, n, dims=(1, 2, 3))
+        assert rel(to_np(o), ref) <= 1e-5
+        key = type(t)
+        if key in first:
+            assert torch.equal(first[key], o), f"{t}: concurrent copies differ"
+        else:
+            first[key] = o
+
+
 def test_budget_admission_and_rejection():
     # host inputs and server-held outputs are staged in the arena: a 1 MiB
     # arena holds at most two 32^3 ComplexF32 requests (2 x 256 KiB each)
