@@ -362,13 +362,17 @@ template <int BAR> __device__ __forceinline__ void stage_sync() {
 // CIN/COUT: the shared-memory views the stage reads and writes (they differ
 // when a stage moves a tile between a dense TMA buffer and a padded one).
 // toff: offset of this stage in a StageTw table (Ns - R_0).
-template <typename T, int R, int BMAX, bool FAST_IO, int SMEM_IO, int BAR, class CIN, class COUT, class TW>
+template <typename T, int R, int BMAX, bool FAST_IO, int SMEM_IO, int BAR, int DIR, class CIN, class COUT, class TW>
 __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int Ns, int ts, int toff,
                                            bool first, bool last, int t, const CIN& cin,
                                            const COUT& cout, const TW& tw, long long ib,
                                            long long ob, bool cv) {
   typedef typename cvec<T>::type V;
   const int Lr = L / R;
+  // direction: at run time (DIR 0), or compiled in (1 forward: no
+  // conjugation, unit scale; 2 inverse)
+  const bool inv = DIR == 0 ? d.inverse != 0 : DIR == 2;
+  const T scale = DIR == 1 ? (T)1 : (T)d.scale;
   const bool to_global = SMEM_IO != 1 && last && !d.epi;
   const bool from_global = SMEM_IO == 0 && first;
   V v[BMAX][R];
@@ -384,11 +388,11 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
           if (!cv) x = mk<V>((T)0, (T)0);
           else if (FAST_IO) x = reinterpret_cast<const V*>(d.in.p)[ib + k * d.in.sk];
           else x = load_elem<T>(d.in, ib, k);
-          if (d.inverse) x.y = -x.y;
+          if (inv) x.y = -x.y;
           v[b][r] = x;
         } else {
           V x = cin.ld(j, r * Lr);
-          if (SMEM_IO != 0 && first && d.inverse) x.y = -x.y;
+          if (SMEM_IO != 0 && first && inv) x.y = -x.y;
           v[b][r] = x;
         }
       }
@@ -412,15 +416,15 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
         if (to_global) {
           if (cv) {
             V y = v[b][r];
-            if (d.inverse) y.y = -y.y;
+            if (inv) y.y = -y.y;
             // SMEM_IO 2 (the fused slab pass) stores whole pencils: unit stride
-            if (FAST_IO) reinterpret_cast<V*>(d.out.p)[ob + (SMEM_IO == 2 ? k : k * d.out.sk)] = cscale(y, (T)d.scale);
-            else store_elem<T>(d.out, ob, k, y, (T)d.scale);
+            if (FAST_IO) reinterpret_cast<V*>(d.out.p)[ob + (SMEM_IO == 2 ? k : k * d.out.sk)] = cscale(y, scale);
+            else store_elem<T>(d.out, ob, k, y, scale);
           }
         } else if (SMEM_IO == 1 && last) {
           V y = v[b][r];
-          if (d.inverse) y.y = -y.y;
-          cout.st(o0, r * Ns, cscale(y, (T)d.scale));
+          if (inv) y.y = -y.y;
+          cout.st(o0, r * Ns, cscale(y, scale));
         } else {
           cout.st(o0, r * Ns, v[b][r]);
         }
@@ -475,7 +479,7 @@ __device__ __forceinline__ void r2c_epilogue(const PassDesc& d, int P, const Col
 
 // Compile-time stage sequence.  The first stage reads CFIRST, the last
 // stage writes CLAST, every other access goes through CMID.
-template <typename T, int L, int P, bool FAST_IO, int SMEM_IO, int BAR, int NS, int R0, int S, class CFIRST,
+template <typename T, int L, int P, bool FAST_IO, int SMEM_IO, int BAR, int DIR, int NS, int R0, int S, class CFIRST,
           class CMID, class CLAST, class TW, int R, int... Rest>
 __device__ __forceinline__ void static_stages(const PassDesc& d, int t, const CFIRST& cf,
                                               const CMID& cm, const CLAST& cl, const TW& tw,
@@ -487,16 +491,16 @@ __device__ __forceinline__ void static_stages(const PassDesc& d, int t, const CF
   constexpr bool LAST = (sizeof...(Rest) == 0);
   constexpr int R0_ = FIRST ? R : R0;
   if constexpr (FIRST && LAST) {
-    stage_body<T, R, BM, FAST_IO, SMEM_IO, BAR>(d, L, P, NS, TS, NS - R0_, true, true, t, cf, cl, tw, ib, ob, cv);
+    stage_body<T, R, BM, FAST_IO, SMEM_IO, BAR, DIR>(d, L, P, NS, TS, NS - R0_, true, true, t, cf, cl, tw, ib, ob, cv);
   } else if constexpr (FIRST) {
-    stage_body<T, R, BM, FAST_IO, SMEM_IO, BAR>(d, L, P, NS, TS, NS - R0_, true, false, t, cf, cm, tw, ib, ob, cv);
+    stage_body<T, R, BM, FAST_IO, SMEM_IO, BAR, DIR>(d, L, P, NS, TS, NS - R0_, true, false, t, cf, cm, tw, ib, ob, cv);
   } else if constexpr (LAST) {
-    stage_body<T, R, BM, FAST_IO, SMEM_IO, BAR>(d, L, P, NS, TS, NS - R0_, false, true, t, cm, cl, tw, ib, ob, cv);
+    stage_body<T, R, BM, FAST_IO, SMEM_IO, BAR, DIR>(d, L, P, NS, TS, NS - R0_, false, true, t, cm, cl, tw, ib, ob, cv);
   } else {
-    stage_body<T, R, BM, FAST_IO, SMEM_IO, BAR>(d, L, P, NS, TS, NS - R0_, false, false, t, cm, cm, tw, ib, ob, cv);
+    stage_body<T, R, BM, FAST_IO, SMEM_IO, BAR, DIR>(d, L, P, NS, TS, NS - R0_, false, false, t, cm, cm, tw, ib, ob, cv);
   }
   if constexpr (sizeof...(Rest) > 0)
-    static_stages<T, L, P, FAST_IO, SMEM_IO, BAR, NS * R, R0_, S + 1, CFIRST, CMID, CLAST, TW, Rest...>(
+    static_stages<T, L, P, FAST_IO, SMEM_IO, BAR, DIR, NS * R, R0_, S + 1, CFIRST, CMID, CLAST, TW, Rest...>(
         d, t, cf, cm, cl, tw, ib, ob, cv);
 }
 
@@ -508,7 +512,7 @@ __global__ void __launch_bounds__(LB) axis_pass_static(const PassDesc d) {
   const ColCtx x = col_ctx(d, P);
   const PadCol<V> col{sm + x.c * d.ld};
   const GlobalTw<V> tw{reinterpret_cast<const V*>(d.tw)};
-  static_stages<T, L, P, FAST_IO, 0, 0, 1, 1, 0, PadCol<V>, PadCol<V>, PadCol<V>, GlobalTw<V>, Rs...>(
+  static_stages<T, L, P, FAST_IO, 0, 0, 0, 1, 1, 0, PadCol<V>, PadCol<V>, PadCol<V>, GlobalTw<V>, Rs...>(
       d, x.t, col, col, col, tw, x.ib, x.ob, x.cv);
   if (!FAST_IO && d.epi) r2c_epilogue<T>(d, P, x, col.p);
 }
@@ -525,11 +529,11 @@ __device__ __noinline__ void dyn_stage(const PassDesc& d, int s, int t, typename
   const PadCol<V> c{col};
   if constexpr (CTW) {
     const ComputedTw<V> g{d.L};
-    stage_body<T, R, EMAX / R, false, 0, 0>(d, d.L, d.P, d.ns[s], d.tws[s], 0, s == 0,
+    stage_body<T, R, EMAX / R, false, 0, 0, 0>(d, d.L, d.P, d.ns[s], d.tws[s], 0, s == 0,
                                              s == d.nst - 1, t, c, c, g, ib, ob, cv);
   } else {
     const GlobalTw<V> g{tw};
-    stage_body<T, R, EMAX / R, false, 0, 0>(d, d.L, d.P, d.ns[s], d.tws[s], 0, s == 0,
+    stage_body<T, R, EMAX / R, false, 0, 0, 0>(d, d.L, d.P, d.ns[s], d.tws[s], 0, s == 0,
                                              s == d.nst - 1, t, c, c, g, ib, ob, cv);
   }
 }

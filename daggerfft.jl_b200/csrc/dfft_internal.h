@@ -71,7 +71,8 @@ struct SlabKernel {
   int cs;   // pencils / columns per tile
   int nb;   // tile buffers
   int dflt; // an untuned plan may pick this variant
-  const void* fn;
+  const void* fn;      // forward
+  const void* fn_inv;  // inverse
 };
 // Variant `v` (0-based) for (dbl, L), or null past the last one.
 const SlabKernel* find_slab_kernel(int dbl, int L, int v = 0);

@@ -294,11 +294,13 @@ static Pass make_feed_pass(const PassSpec& s) {
   const SlabKernel* k = find_strided_kernel(s.dbl, L, s.C < 0 ? 0 : s.C);
   if (!k) throw Error{DFFT_ERROR_INVALID_VALUE, "no such strided launch shape"};
   if (s.I < k->cs) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "fewer columns than one tile"};
+  // the forward kernels have conjugation off and unit scale compiled in
+  if (!s.inverse && s.scale != 1.0) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "scaled forward strided pass"};
   const std::vector<int> rad(k->radix, k->radix + k->nst);
   Pass p;
   p.feed = true;
   p.is_static = true;
-  p.fn = k->fn;
+  p.fn = s.inverse ? k->fn_inv : k->fn;
   PassDesc& d = p.d;
   d.L = L;
   d.nst = k->nst;
@@ -572,7 +574,7 @@ Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v) {
   Pass p;
   p.slab = true;
   p.is_static = true;
-  p.fn = k->fn;
+  p.fn = inverse ? k->fn_inv : k->fn;
   int ld = swz_host(L - 1, esz) + 1;
   if ((ld & 1) == 0) ld += 1;
   auto fill = [&](PassDesc& d, long long I) {

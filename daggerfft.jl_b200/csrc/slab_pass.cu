@@ -6,10 +6,16 @@
 
 namespace dfft {
 
-#define DFFT_SLAB_INST(T, LB, MINB, NB, L, P, CS, ...)                                                 \
-  template __global__ void slab_xy_pass<T, LB, MINB, NB, L, P, CS, __VA_ARGS__>(                     \
+#define DFFT_SLAB_INST1(T, LB, MINB, NB, DIR, L, P, CS, ...)                                          \
+  template __global__ void slab_xy_pass<T, LB, MINB, NB, DIR, L, P, CS, __VA_ARGS__>(                \
       const PassDesc, const PassDesc, const __grid_constant__ CUtensorMap, const SlabGeom);
-#define K(T, LB, MINB, NB, L, P, CS, ...) (const void*)&slab_xy_pass<T, LB, MINB, NB, L, P, CS, __VA_ARGS__>
+#define DFFT_SLAB_INST(T, LB, MINB, NB, L, P, CS, ...)            \
+  DFFT_SLAB_INST1(T, LB, MINB, NB, 1, L, P, CS, __VA_ARGS__)       \
+  DFFT_SLAB_INST1(T, LB, MINB, NB, 2, L, P, CS, __VA_ARGS__)
+// forward and inverse kernels of one launch shape
+#define K(T, LB, MINB, NB, L, P, CS, ...)                                     \
+  (const void*)&slab_xy_pass<T, LB, MINB, NB, 1, L, P, CS, __VA_ARGS__>,     \
+      (const void*)&slab_xy_pass<T, LB, MINB, NB, 2, L, P, CS, __VA_ARGS__>
 
 // threads = CS*P stage threads + one producer warp; MINB = CTAs per SM that
 // the NB tile buffers of CS*L elements leave room for
@@ -39,7 +45,7 @@ DFFT_SLAB_INST(double, 96, 3, 3, 256, 16, 4, 16, 16)
 // L = 128 the per-axis passes are faster, so only DFFT_FLAG_TUNE or
 // DFFT_FLAG_FUSE selects the fused kernel there).
 static const SlabKernel kSlabKernels[] = {
-    // dbl, L, P, nst, radices, threads, CS, NB, dflt, kernel
+    // dbl, L, P, nst, radices, threads, CS, NB, dflt, forward and inverse kernels
     {0, 512, 32, 3, {8, 8, 8}, 160, 4, 2, 1, K(float, 160, 6, 2, 512, 32, 4, 8, 8, 8)},
     {0, 512, 32, 3, {8, 8, 8}, 160, 4, 2, 1, K(float, 160, 5, 2, 512, 32, 4, 8, 8, 8)},
     {0, 512, 32, 3, {8, 8, 8}, 160, 4, 3, 1, K(float, 160, 4, 3, 512, 32, 4, 8, 8, 8)},

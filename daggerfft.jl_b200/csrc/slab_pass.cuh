@@ -125,7 +125,8 @@ template <int R, int... Rest> struct first_radix { static constexpr int value = 
 // (byte 32), the stage threads' abort flag (byte 64) and the buffers' job
 // records (byte 80); stage twiddles; NB tile buffers.
 // MINB: CTAs per SM the tile buffers allow (register budget per thread).
-template <typename T, int LB, int MINB, int NB, int L, int P, int CS, int... Rs>
+// DIR: 1 forward, 2 inverse (compiled in: no per-element direction tests).
+template <typename T, int LB, int MINB, int NB, int DIR, int L, int P, int CS, int... Rs>
 __global__ void __launch_bounds__(LB, MINB)
     slab_xy_pass(const PassDesc dx, const PassDesc dy, const __grid_constant__ CUtensorMap tout,
                  const SlabGeom g) {
@@ -270,14 +271,14 @@ __global__ void __launch_bounds__(LB, MINB)
         const StrideCol<V> dense{buf + (size_t)c * L, 1};
         const XSwzCol<V, L, R0> sw{buf + (size_t)c * L, c};
         const long long ob = ((long long)J.slab * L + (long long)J.tile * CS + c) * L;
-        static_stages<T, L, P, true, 2, NC, 1, 1, 0, StrideCol<V>, XSwzCol<V, L, R0>, XSwzCol<V, L, R0>,
+        static_stages<T, L, P, true, 2, NC, DIR, 1, 1, 0, StrideCol<V>, XSwzCol<V, L, R0>, XSwzCol<V, L, R0>,
                       StageTw<V>, Rs...>(dx, t, dense, sw, sw, tw, 0, ob, true);
         fence_proxy_async_global();  // these stores are read by bulk-tensor loads
       } else {
         const int c = tid % CS, t = tid / CS;
         const StrideColC<V, CS> dense{buf + c};
         const YSwzCol<V, CS, R0> sw{buf + c};
-        static_stages<T, L, P, true, 1, NC, 1, 1, 0, StrideColC<V, CS>, YSwzCol<V, CS, R0>, StrideColC<V, CS>,
+        static_stages<T, L, P, true, 1, NC, DIR, 1, 1, 0, StrideColC<V, CS>, YSwzCol<V, CS, R0>, StrideColC<V, CS>,
                       StageTw<V>, Rs...>(dy, t, dense, sw, dense, tw, 0, 0, true);
       }
       fence_proxy_async_smem();  // the buffer is next read (store) or written (load) by TMA
@@ -323,7 +324,7 @@ struct StridedGeom {
   int* err;
 };
 
-template <typename T, int LB, int MINB, int NB, int L, int P, int CS, int... Rs>
+template <typename T, int LB, int MINB, int NB, int DIR, int L, int P, int CS, int... Rs>
 __global__ void __launch_bounds__(LB, MINB)
     axis_pass_strided(const PassDesc d, const __grid_constant__ CUtensorMap tin,
                       const __grid_constant__ CUtensorMap tout, const StridedGeom g) {
@@ -409,7 +410,7 @@ __global__ void __launch_bounds__(LB, MINB)
       V* buf = bufs + b * bst;
       const StrideColC<V, CS> dense{buf + c};
       const YSwzCol<V, CS, R0> sw{buf + c};
-      static_stages<T, L, P, true, 1, NC, 1, 1, 0, StrideColC<V, CS>, YSwzCol<V, CS, R0>, StrideColC<V, CS>,
+      static_stages<T, L, P, true, 1, NC, DIR, 1, 1, 0, StrideColC<V, CS>, YSwzCol<V, CS, R0>, StrideColC<V, CS>,
                     StageTw<V>, Rs...>(d, t, dense, sw, dense, tw, 0, 0, true);
       fence_proxy_async_smem();
       stage_sync<NC>();

@@ -6,11 +6,17 @@
 
 namespace dfft {
 
-#define DFFT_STRIDED_INST(T, LB, MINB, NB, L, P, CS, ...)                                              \
-  template __global__ void axis_pass_strided<T, LB, MINB, NB, L, P, CS, __VA_ARGS__>(                \
+#define DFFT_STRIDED_INST1(T, LB, MINB, NB, DIR, L, P, CS, ...)                                       \
+  template __global__ void axis_pass_strided<T, LB, MINB, NB, DIR, L, P, CS, __VA_ARGS__>(           \
       const PassDesc, const __grid_constant__ CUtensorMap, const __grid_constant__ CUtensorMap,       \
       const StridedGeom);
-#define K(T, LB, MINB, NB, L, P, CS, ...) (const void*)&axis_pass_strided<T, LB, MINB, NB, L, P, CS, __VA_ARGS__>
+#define DFFT_STRIDED_INST(T, LB, MINB, NB, L, P, CS, ...)          \
+  DFFT_STRIDED_INST1(T, LB, MINB, NB, 1, L, P, CS, __VA_ARGS__)     \
+  DFFT_STRIDED_INST1(T, LB, MINB, NB, 2, L, P, CS, __VA_ARGS__)
+// forward and inverse kernels of one launch shape
+#define K(T, LB, MINB, NB, L, P, CS, ...)                                          \
+  (const void*)&axis_pass_strided<T, LB, MINB, NB, 1, L, P, CS, __VA_ARGS__>,     \
+      (const void*)&axis_pass_strided<T, LB, MINB, NB, 2, L, P, CS, __VA_ARGS__>
 
 // ComplexF32, L = 512 (8 x 8 x 8)
 DFFT_STRIDED_INST(float, 288, 3, 2, 512, 32, 8, 8, 8, 8)
@@ -30,7 +36,7 @@ DFFT_STRIDED_INST(double, 160, 3, 2, 256, 16, 8, 16, 16)
 DFFT_STRIDED_INST(double, 96, 5, 2, 256, 16, 4, 16, 16)
 
 static const SlabKernel kStridedKernels[] = {
-    // dbl, L, P, nst, radices, threads, CS, NB, dflt, kernel
+    // dbl, L, P, nst, radices, threads, CS, NB, dflt, forward and inverse kernels
     {0, 512, 32, 3, {8, 8, 8}, 288, 8, 3, 1, K(float, 288, 2, 3, 512, 32, 8, 8, 8, 8)},
     {0, 512, 32, 3, {8, 8, 8}, 288, 8, 2, 1, K(float, 288, 3, 2, 512, 32, 8, 8, 8, 8)},
     {0, 512, 32, 3, {8, 8, 8}, 160, 4, 2, 1, K(float, 160, 6, 2, 512, 32, 4, 8, 8, 8)},

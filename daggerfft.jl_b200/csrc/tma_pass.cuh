@@ -239,16 +239,16 @@ __global__ void __launch_bounds__(LB) axis_pass_pipe(const PassDesc d,
     if (CONTIG) {
       const StrideCol<V> dense{sb + (size_t)c * L, 1};
       const PadCol<V> pad{work + (size_t)c * g.ld};
-      static_stages<T, L, P, true, 1, 0, 1, 1, 0, StrideCol<V>, PadCol<V>, StrideCol<V>, StageTw<V>,
+      static_stages<T, L, P, true, 1, 0, 0, 1, 1, 0, StrideCol<V>, PadCol<V>, StrideCol<V>, StageTw<V>,
                     Rs...>(d, t, dense, pad, dense, tw, 0, 0, true);
     } else {
       if constexpr (CS > 0) {
         const StrideColC<V, CS> col{sb + c};
-        static_stages<T, L, P, true, 1, 0, 1, 1, 0, StrideColC<V, CS>, StrideColC<V, CS>,
+        static_stages<T, L, P, true, 1, 0, 0, 1, 1, 0, StrideColC<V, CS>, StrideColC<V, CS>,
                       StrideColC<V, CS>, GlobalTw<V>, Rs...>(d, t, col, col, col, twl, 0, 0, true);
       } else {
         const StrideCol<V> col{sb + c, C};
-        static_stages<T, L, P, true, 1, 0, 1, 1, 0, StrideCol<V>, StrideCol<V>, StrideCol<V>,
+        static_stages<T, L, P, true, 1, 0, 0, 1, 1, 0, StrideCol<V>, StrideCol<V>, StrideCol<V>,
                       GlobalTw<V>, Rs...>(d, t, col, col, col, twl, 0, 0, true);
       }
     }
