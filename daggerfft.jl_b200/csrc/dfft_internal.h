@@ -5,7 +5,7 @@
 #include <memory>
 #include <string>
 #include <vector>
-#include "slab_pass.cuh"
+#include "real_pass.cuh"
 
 namespace dfft {
 
@@ -56,6 +56,8 @@ struct Pass {
   bool slab = false;
   bool feed = false;     // axis_pass_strided (tensor maps as for tma)
   StridedGeom fgeom{};
+  bool real = false;     // real_pass (R2C / C2R along the contiguous axis)
+  RealGeom rgeom{};
   size_t ctr_bytes = 0;  // job and per-slab counters (in the plan workspace)
   PassDesc d2{};
   SlabGeom sgeom{};
@@ -78,6 +80,8 @@ struct SlabKernel {
 const SlabKernel* find_slab_kernel(int dbl, int L, int v = 0);
 // Launch shapes of axis_pass_strided for (dbl, L), same conventions.
 const SlabKernel* find_strided_kernel(int dbl, int L, int v = 0);
+// real_pass kernels for half length M (fn: R2C, fn_inv: C2R), or null.
+const SlabKernel* find_real_kernel(int dbl, int M);
 
 // Fused forward or inverse 2-D C2C over dims 1 and 2 of an L x L x O array
 // (scales: 1 forward, 1/L per axis inverse) with launch variant v; throws

@@ -360,8 +360,94 @@ static Pass make_feed_pass(const PassSpec& s) {
   return p;
 }
 
+// R2C first pass / C2R last pass over whole contiguous pencils (I = 1):
+// real_pass when a kernel exists for the half length and the pencils split
+// into whole tiles.
+static int real_kind(const PassSpec& s) {
+  const long long L = s.L;
+  if (s.I != 1 || s.in.sk != 1 || s.out.sk != 1 || s.in.chirp || s.out.chirp || s.in.mul || s.out.mul) return 0;
+  if (s.epi && !s.inverse && s.in.kind == IO_REAL_PAIR && s.out.kind == IO_CPLX && s.in.so == 2 * L &&
+      s.out.so == L + 1)
+    return 1;
+  if (!s.epi && s.inverse && s.in.kind == IO_HERM_PAIR && s.out.kind == IO_REAL_PAIR && s.in.so == L + 1 &&
+      s.in.n == L && s.out.so == 2 * L)
+    return 2;
+  return 0;
+}
+
+static Pass make_real_pass(const PassSpec& s) {
+  const int kind = real_kind(s);
+  const int M = s.L;
+  const int esz = s.dbl ? 16 : 8;
+  const SlabKernel* k = kind ? find_real_kernel(s.dbl, M) : nullptr;
+  if (!k) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "no pipelined real kernel for this pass"};
+  if (s.O % k->cs != 0) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "pencils do not split into whole tiles"};
+  const std::vector<int> rad(k->radix, k->radix + k->nst);
+  Pass p;
+  p.real = true;
+  p.is_static = true;
+  p.fn = kind == 1 ? k->fn : k->fn_inv;
+  PassDesc& d = p.d;
+  d.L = M;
+  d.nst = k->nst;
+  int ns = 1;
+  for (int i = 0; i < d.nst; ++i) {
+    d.radix[i] = rad[i];
+    d.ns[i] = ns;
+    d.tws[i] = M / (ns * rad[i]);
+    ns *= rad[i];
+  }
+  int ld = swz_host(M - 1, esz) + 1;
+  if ((ld & 1) == 0) ld += 1;
+  d.P = k->P;
+  d.C = k->cs;
+  d.ld = ld;
+  d.inverse = kind == 2 ? 1 : 0;
+  d.cfast = 0;
+  d.epi = 0;
+  d.Q = s.O;
+  d.I = 1;
+  d.scale = s.scale;
+  d.in = s.in;
+  d.out = s.out;
+  for (auto& t : s.keep) p.tables.push_back(t);
+  auto stw = stage_twiddles(s.dbl, M, rad);
+  p.tables.push_back(stw);
+  d.tw = stw->p;
+  auto w = twiddle_table(s.dbl, 2LL * M, 1, 0, M + 1, false);
+  p.tables.push_back(w);
+  d.tw2 = w->p;
+  RealGeom& g = p.rgeom;
+  g.ntiles = s.O / k->cs;
+  g.ntw = k->nst > 1 ? M - rad[0] : 0;
+  g.ld = ld;
+  const size_t bstride = ((size_t)k->cs * (M + 1) * esz + 127) & ~(size_t)127;
+  g.bstride = (int)(bstride / esz);
+  g.err = device_error_word();
+  const size_t tw_bytes = ((size_t)(g.ntw + M + 1) * esz + 127) & ~(size_t)127;
+  p.smem = kSlabHeader + tw_bytes + (size_t)k->nb * bstride + (size_t)k->cs * ld * esz;
+  p.block = dim3((unsigned)k->lb);
+  if (p.smem > max_smem_per_block()) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "real tiles do not fit"};
+  cuda_check(ensure_smem_attr(p.fn, p.smem), "cudaFuncSetAttribute(real)");
+  int occ = 0;
+  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p.fn, (int)p.block.x, p.smem),
+             "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (occ < 1) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "real kernel cannot be resident"};
+  long long nb = (long long)sm_count() * occ;
+  if (nb > g.ntiles) nb = g.ntiles;
+  p.grid = dim3((unsigned)(nb > 0 ? nb : 1));
+  return p;
+}
+
 Pass make_pass(const PassSpec& s) {
   if (s.variant == VARIANT_FEED) return make_feed_pass(s);
+  if (s.variant == VARIANT_AUTO && real_kind(s)) {
+    try {
+      return make_real_pass(s);
+    } catch (const Error& e) {
+      if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
+    }
+  }
   Pass p;
   PassDesc& d = p.d;
   const int L = s.L;
@@ -658,6 +744,13 @@ cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream,
   PassDesc d = p.d;
   d.in.p = in;
   d.out.p = out;
+  if (p.real) {
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
+      return cudaErrorMisalignedAddress;
+    RealGeom g = p.rgeom;
+    void* args[] = {&d, &g};
+    return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
+  }
   if (p.feed) {
     if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
       return cudaErrorMisalignedAddress;
