@@ -110,6 +110,68 @@ template <typename V> __device__ __forceinline__ V ldg_c(const V* p) { return __
 //   DHT       N           x_n                                   Y_k = Re X_k - Im X_k
 // ---------------------------------------------------------------------------
 
+// One FFTW r2r kind's load map (element k of the FFT input, from real data
+// of extent N at p[b + n*sk]) and store map (FFT output element k, scaled
+// by s, into the real result); w is the kind's twiddle table.
+template <typename T, int KIND>
+__device__ __forceinline__ typename cvec<T>::type r2r_load(const T* p, long long b, long long sk, int N,
+                                                         const typename cvec<T>::type* w, int k) {
+  typedef typename cvec<T>::type V;
+  const T z = (T)0;
+  if constexpr (KIND == K_REDFT10 || KIND == K_RODFT10) {
+    const int n = (2 * k < N) ? 2 * k : 2 * N - 2 * k - 1;
+    T v = p[b + n * sk];
+    if (KIND == K_RODFT10 && (n & 1)) v = -v;
+    return mk<V>(v, z);
+  } else if constexpr (KIND == K_REDFT01 || KIND == K_RODFT01) {
+    const bool rev = (KIND == K_RODFT01);
+    const T a = p[b + (rev ? N - 1 - k : k) * sk];
+    const T c = (k == 0) ? z : p[b + (rev ? k - 1 : N - k) * sk];
+    return cmul(ldg_c(w + k), mk<V>(a, -c));
+  } else if constexpr (KIND == K_REDFT11 || KIND == K_RODFT11) {
+    if (k >= N) return mk<V>(z, z);
+    const T a = p[b + (KIND == K_RODFT11 ? N - 1 - k : k) * sk];
+    const V t = ldg_c(w + k);
+    return mk<V>(a * t.x, a * t.y);
+  } else if constexpr (KIND == K_REDFT00) {
+    const int n = (k < N) ? k : 2 * (N - 1) - k;
+    return mk<V>(p[b + n * sk], z);
+  } else if constexpr (KIND == K_RODFT00) {
+    if (k == 0 || k == N + 1) return mk<V>(z, z);
+    if (k <= N) return mk<V>(p[b + (k - 1) * sk], z);
+    return mk<V>(-p[b + (2 * N + 1 - k) * sk], z);
+  } else {  // K_DHT
+    return mk<V>(p[b + k * sk], z);
+  }
+}
+
+template <typename T, int KIND>
+__device__ __forceinline__ void r2r_store(T* p, long long b, long long sk, int N, const typename cvec<T>::type* w,
+                                          int k, typename cvec<T>::type v, T s) {
+  typedef typename cvec<T>::type V;
+  if constexpr (KIND == K_REDFT10 || KIND == K_RODFT10) {
+    const V t = ldg_c(w + k);
+    p[b + (KIND == K_RODFT10 ? N - 1 - k : k) * sk] = (T)2 * (v.x * t.x - v.y * t.y) * s;
+  } else if constexpr (KIND == K_REDFT01 || KIND == K_RODFT01) {
+    const int n = (2 * k < N) ? 2 * k : 2 * N - 2 * k - 1;
+    T y = v.x * s;
+    if (KIND == K_RODFT01 && (n & 1)) y = -y;
+    p[b + n * sk] = y;
+  } else if constexpr (KIND == K_REDFT11 || KIND == K_RODFT11) {
+    if (k >= N) return;
+    const V t = ldg_c(w + k);
+    T y = (T)2 * (v.x * t.x - v.y * t.y) * s;
+    if (KIND == K_RODFT11 && (k & 1)) y = -y;
+    p[b + k * sk] = y;
+  } else if constexpr (KIND == K_REDFT00) {
+    if (k < N) p[b + k * sk] = v.x * s;
+  } else if constexpr (KIND == K_RODFT00) {
+    if (k >= 1 && k <= N) p[b + (k - 1) * sk] = -v.y * s;
+  } else {  // K_DHT
+    p[b + k * sk] = (v.x - v.y) * s;
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ typename cvec<T>::type load_raw(const IoAny& io, long long b, int k) {
   typedef typename cvec<T>::type V;
@@ -150,41 +212,16 @@ __device__ __forceinline__ typename cvec<T>::type load_raw(const IoAny& io, long
     default: {  // IO_R2R
       const T* p = reinterpret_cast<const T*>(io.p);
       const V* w = reinterpret_cast<const V*>(io.w);
-      const int N = io.n;
-      const long long sk = io.sk;
       switch (io.r2r) {
-        case K_REDFT10:
-        case K_RODFT10: {
-          const int n = (2 * k < N) ? 2 * k : 2 * N - 2 * k - 1;
-          T v = p[b + n * sk];
-          if (io.r2r == K_RODFT10 && (n & 1)) v = -v;
-          return mk<V>(v, z);
-        }
-        case K_REDFT01:
-        case K_RODFT01: {
-          const bool rev = (io.r2r == K_RODFT01);
-          const T a = p[b + (rev ? N - 1 - k : k) * sk];
-          const T c = (k == 0) ? z : p[b + (rev ? k - 1 : N - k) * sk];
-          return cmul(ldg_c(w + k), mk<V>(a, -c));
-        }
-        case K_REDFT11:
-        case K_RODFT11: {
-          if (k >= N) return mk<V>(z, z);
-          const T a = p[b + (io.r2r == K_RODFT11 ? N - 1 - k : k) * sk];
-          const V t = ldg_c(w + k);
-          return mk<V>(a * t.x, a * t.y);
-        }
-        case K_REDFT00: {
-          const int n = (k < N) ? k : 2 * (N - 1) - k;
-          return mk<V>(p[b + n * sk], z);
-        }
-        case K_RODFT00: {
-          if (k == 0 || k == N + 1) return mk<V>(z, z);
-          if (k <= N) return mk<V>(p[b + (k - 1) * sk], z);
-          return mk<V>(-p[b + (2 * N + 1 - k) * sk], z);
-        }
-        default:  // K_DHT
-          return mk<V>(p[b + k * sk], z);
+        case K_REDFT10: return r2r_load<T, K_REDFT10>(p, b, io.sk, io.n, w, k);
+        case K_RODFT10: return r2r_load<T, K_RODFT10>(p, b, io.sk, io.n, w, k);
+        case K_REDFT01: return r2r_load<T, K_REDFT01>(p, b, io.sk, io.n, w, k);
+        case K_RODFT01: return r2r_load<T, K_RODFT01>(p, b, io.sk, io.n, w, k);
+        case K_REDFT11: return r2r_load<T, K_REDFT11>(p, b, io.sk, io.n, w, k);
+        case K_RODFT11: return r2r_load<T, K_RODFT11>(p, b, io.sk, io.n, w, k);
+        case K_REDFT00: return r2r_load<T, K_REDFT00>(p, b, io.sk, io.n, w, k);
+        case K_RODFT00: return r2r_load<T, K_RODFT00>(p, b, io.sk, io.n, w, k);
+        default: return r2r_load<T, K_DHT>(p, b, io.sk, io.n, w, k);
       }
     }
   }
@@ -214,41 +251,16 @@ __device__ __forceinline__ void store_raw(const IoAny& io, long long b, int k,
     default: {  // IO_R2R
       T* p = reinterpret_cast<T*>(io.p);
       const V* w = reinterpret_cast<const V*>(io.w);
-      const int N = io.n;
-      const long long sk = io.sk;
       switch (io.r2r) {
-        case K_REDFT10:
-        case K_RODFT10: {
-          const V t = ldg_c(w + k);
-          p[b + (io.r2r == K_RODFT10 ? N - 1 - k : k) * sk] = (T)2 * (v.x * t.x - v.y * t.y) * s;
-          return;
-        }
-        case K_REDFT01:
-        case K_RODFT01: {
-          const int n = (2 * k < N) ? 2 * k : 2 * N - 2 * k - 1;
-          T y = v.x * s;
-          if (io.r2r == K_RODFT01 && (n & 1)) y = -y;
-          p[b + n * sk] = y;
-          return;
-        }
-        case K_REDFT11:
-        case K_RODFT11: {
-          if (k >= N) return;
-          const V t = ldg_c(w + k);
-          T y = (T)2 * (v.x * t.x - v.y * t.y) * s;
-          if (io.r2r == K_RODFT11 && (k & 1)) y = -y;
-          p[b + k * sk] = y;
-          return;
-        }
-        case K_REDFT00:
-          if (k < N) p[b + k * sk] = v.x * s;
-          return;
-        case K_RODFT00:
-          if (k >= 1 && k <= N) p[b + (k - 1) * sk] = -v.y * s;
-          return;
-        default:  // K_DHT
-          p[b + k * sk] = (v.x - v.y) * s;
-          return;
+        case K_REDFT10: r2r_store<T, K_REDFT10>(p, b, io.sk, io.n, w, k, v, s); return;
+        case K_RODFT10: r2r_store<T, K_RODFT10>(p, b, io.sk, io.n, w, k, v, s); return;
+        case K_REDFT01: r2r_store<T, K_REDFT01>(p, b, io.sk, io.n, w, k, v, s); return;
+        case K_RODFT01: r2r_store<T, K_RODFT01>(p, b, io.sk, io.n, w, k, v, s); return;
+        case K_REDFT11: r2r_store<T, K_REDFT11>(p, b, io.sk, io.n, w, k, v, s); return;
+        case K_RODFT11: r2r_store<T, K_RODFT11>(p, b, io.sk, io.n, w, k, v, s); return;
+        case K_REDFT00: r2r_store<T, K_REDFT00>(p, b, io.sk, io.n, w, k, v, s); return;
+        case K_RODFT00: r2r_store<T, K_RODFT00>(p, b, io.sk, io.n, w, k, v, s); return;
+        default: r2r_store<T, K_DHT>(p, b, io.sk, io.n, w, k, v, s); return;
       }
     }
   }

@@ -78,6 +78,7 @@ int dfft_plan_describe(dfft_plan plan, char* buf, size_t len) {
     std::string out;
     for (const dfft::Pass& q : p->passes) {
       const char* kind = q.slab ? "slab-xy" : q.feed ? "strided-feed" : q.real ? "real-pipe"
+                         : q.tiled == 1 ? "tiled-contig" : q.tiled == 2 ? "tiled-strided"
                          : q.pipe ? (q.tma ? "strided-pipe" : "contig-pipe")
                          : q.is_static ? "direct" : "dynamic";
       char line[256];

@@ -5,7 +5,7 @@
 #include <memory>
 #include <string>
 #include <vector>
-#include "real_pass.cuh"
+#include "tiled_pass.cuh"
 
 namespace dfft {
 
@@ -58,6 +58,9 @@ struct Pass {
   StridedGeom fgeom{};
   bool real = false;     // real_pass (R2C / C2R along the contiguous axis)
   RealGeom rgeom{};
+  int tiled = 0;         // tiled_pass: 1 contiguous, 2 strided (real tensor maps)
+  int tdbl = 0;          // its precision (element type of the tensor maps)
+  TiledGeom tgeom{};
   size_t ctr_bytes = 0;  // job and per-slab counters (in the plan workspace)
   PassDesc d2{};
   SlabGeom sgeom{};
@@ -82,6 +85,16 @@ const SlabKernel* find_slab_kernel(int dbl, int L, int v = 0);
 const SlabKernel* find_strided_kernel(int dbl, int L, int v = 0);
 // real_pass kernels for half length M (fn: R2C, fn_inv: C2R), or null.
 const SlabKernel* find_real_kernel(int dbl, int M);
+// A compiled tiled_pass (tiled_pass.cu).
+struct TiledKernel {
+  int dbl, L, P, nst, radix[4];
+  int lb;       // threads per CTA
+  int cs;       // pencils / columns per tile
+  int strided;  // 0 contiguous axis, 1 strided axis
+  int kind;     // FFTW r2r kind (REDFT10 / REDFT01)
+  const void* fn;
+};
+const TiledKernel* find_tiled_kernel(int dbl, int L, int strided, int kind);
 
 // Fused forward or inverse 2-D C2C over dims 1 and 2 of an L x L x O array
 // (scales: 1 forward, 1/L per axis inverse) with launch variant v; throws

@@ -183,6 +183,21 @@ int* device_error_word() {
   return w;
 }
 
+// Tensor map over the real tensor {I, n, O} of a strided tiled pass.
+static cudaError_t encode_real_map(CUtensorMap* m, void* base, const Pass& p, int dbl) {
+  std::call_once(g_encode_once, load_encode);
+  if (!g_encode) return cudaErrorNotSupported;
+  const cuuint64_t esz = dbl ? 8 : 4;
+  cuuint64_t dims[3] = {(cuuint64_t)p.tI, (cuuint64_t)p.tL, (cuuint64_t)p.tO};
+  cuuint64_t strides[2] = {(cuuint64_t)p.tI * esz, (cuuint64_t)p.tI * esz * (cuuint64_t)p.tL};
+  cuuint32_t box[3] = {(cuuint32_t)p.geom.C, (cuuint32_t)p.geom.lb, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = g_encode(m, dbl ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims,
+                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 static cudaError_t encode_map(CUtensorMap* m, void* base, const Pass& p) {
   std::call_once(g_encode_once, load_encode);
   if (!g_encode) return cudaErrorNotSupported;
@@ -439,8 +454,110 @@ static Pass make_real_pass(const PassSpec& s) {
   return p;
 }
 
+// R2R passes whose tiles are whole contiguous pencils (1) or strided
+// columns (2) of the real data: tiled_pass.
+static int tiled_kind(const PassSpec& s) {
+  if (s.in.kind != IO_R2R || s.out.kind != IO_R2R || s.epi || s.in.chirp || s.out.chirp || s.in.mul ||
+      s.out.mul || s.in.n != s.out.n || s.in.r2r != s.out.r2r ||
+      (s.in.r2r != K_REDFT10 && s.in.r2r != K_REDFT01))
+    return 0;
+  const long long n = s.in.n;
+  if (s.I == 1 && s.in.sk == 1 && s.out.sk == 1 && s.in.so == n && s.out.so == n) return 1;
+  if (s.I > 1 && s.in.sk == s.I && s.out.sk == s.I && s.in.so == s.I * n && s.out.so == s.I * n) return 2;
+  return 0;
+}
+
+static Pass make_tiled_pass(const PassSpec& s) {
+  const int kind = tiled_kind(s);
+  const int L = s.L;
+  const int rsz = s.dbl ? 8 : 4, csz = 2 * rsz;
+  const TiledKernel* k = kind ? find_tiled_kernel(s.dbl, L, kind == 2 ? 1 : 0, s.in.r2r) : nullptr;
+  if (!k) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "no tiled kernel for this pass"};
+  const int n = s.in.n;
+  const int C = k->cs;
+  Pass p;
+  p.tiled = kind;
+  p.tdbl = s.dbl;
+  p.is_static = true;
+  p.fn = k->fn;
+  TiledGeom& g = p.tgeom;
+  g.n_in = g.n_out = n;
+  if (kind == 1) {
+    if (s.O % C != 0 || ((size_t)C * n * rsz) % 16 != 0)
+      throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "pencils do not split into whole tiles"};
+    g.ntiles = s.O / C;
+    g.tiles_i = 1;
+    g.lb = n;
+    g.nlb = 1;
+  } else {
+    if (s.I < C || (s.I * rsz) % 16 != 0 || ((size_t)C * rsz) % 16 != 0 || s.I >= (1LL << 31) ||
+        s.O >= (1LL << 31))
+      throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "columns cannot be tiled by TMA"};
+    g.tiles_i = (int)((s.I + C - 1) / C);
+    g.ntiles = (long long)g.tiles_i * s.O;
+    g.lb = box_rows(n);
+    g.nlb = n / g.lb;
+    if (g.nlb > 16 || (g.nlb > 1 && ((size_t)g.lb * C * rsz) % 128 != 0))
+      throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "rows cannot be split into TMA boxes"};
+    p.geom.C = C;
+    p.geom.lb = g.lb;
+    p.tI = s.I;
+    p.tL = n;
+    p.tO = s.O;
+  }
+  PassDesc& d = p.d;
+  d.L = L;
+  d.nst = k->nst;
+  int ns = 1;
+  for (int i = 0; i < d.nst; ++i) {
+    d.radix[i] = k->radix[i];
+    d.ns[i] = ns;
+    d.tws[i] = L / (ns * k->radix[i]);
+    ns *= k->radix[i];
+  }
+  int ld = swz_host(L - 1, csz) + 1;
+  if ((ld & 1) == 0) ld += 1;
+  d.P = k->P;
+  d.C = C;
+  d.ld = ld;
+  d.inverse = s.inverse;
+  d.cfast = kind == 2 ? 1 : 0;
+  d.epi = 0;
+  d.Q = s.I * s.O;
+  d.I = s.I;
+  d.scale = s.scale;
+  d.in = s.in;
+  d.out = s.out;
+  for (auto& t : s.keep) p.tables.push_back(t);
+  auto tw = twiddle_table(s.dbl, L, 1, 0, L, false);
+  p.tables.push_back(tw);
+  d.tw = tw->p;
+  g.ld = ld;
+  g.bstride = (int)(((size_t)C * n * rsz + 127) & ~(size_t)127);
+  g.err = device_error_word();
+  p.smem = kSlabHeader + 2 * (size_t)g.bstride + (size_t)C * ld * csz;
+  p.block = dim3((unsigned)k->lb);
+  if (p.smem > max_smem_per_block()) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "tiles do not fit"};
+  cuda_check(ensure_smem_attr(p.fn, p.smem), "cudaFuncSetAttribute(tiled)");
+  int occ = 0;
+  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p.fn, (int)p.block.x, p.smem),
+             "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (occ < 1) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "tiled kernel cannot be resident"};
+  long long nb = (long long)sm_count() * occ;
+  if (nb > g.ntiles) nb = g.ntiles;
+  p.grid = dim3((unsigned)(nb > 0 ? nb : 1));
+  return p;
+}
+
 Pass make_pass(const PassSpec& s) {
   if (s.variant == VARIANT_FEED) return make_feed_pass(s);
+  if (s.variant == VARIANT_AUTO && tiled_kind(s)) {
+    try {
+      return make_tiled_pass(s);
+    } catch (const Error& e) {
+      if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
+    }
+  }
   if (s.variant == VARIANT_AUTO && real_kind(s)) {
     try {
       return make_real_pass(s);
@@ -744,6 +861,24 @@ cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream,
   PassDesc d = p.d;
   d.in.p = in;
   d.out.p = out;
+  if (p.tiled) {
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
+      return cudaErrorMisalignedAddress;
+    CUtensorMap tin, tout;
+    std::memset(&tin, 0, sizeof(tin));
+    std::memset(&tout, 0, sizeof(tout));
+    if (p.tiled == 2) {
+      e = encode_real_map(&tin, in, p, p.tdbl);
+      if (e != cudaSuccess) return e;
+      e = encode_real_map(&tout, out, p, p.tdbl);
+      if (e != cudaSuccess) return e;
+    }
+    TiledGeom g = p.tgeom;
+    g.src = in;
+    g.dst = out;
+    void* args[] = {&d, &tin, &tout, &g};
+    return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
+  }
   if (p.real) {
     if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
       return cudaErrorMisalignedAddress;
