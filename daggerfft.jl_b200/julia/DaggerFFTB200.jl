@@ -34,6 +34,9 @@ code(::FFT!) = Cint(4); code(::IFFT!) = Cint(5); code(::RFFT!) = Cint(6); code(:
 code(::R2R) = Cint(8)
 
 # FFTW r2r kind values
+# plan flags (dfft.h)
+const FLAG_DESTROY_INPUT = Cuint(1); const FLAG_TUNE = Cuint(2); const FLAG_NO_WISDOM = Cuint(4)
+const FLAG_NO_FUSE = Cuint(8); const FLAG_FUSE = Cuint(16)
 const DHT = 2; const REDFT00 = 3; const REDFT01 = 4; const REDFT10 = 5; const REDFT11 = 6
 const RODFT00 = 7; const RODFT01 = 8; const RODFT10 = 9; const RODFT11 = 10
 
@@ -80,6 +83,13 @@ function plan_transform(transform, A::CuArray, dims; decomp=Pencil(), n=0, metho
         check(ccall((:dfft_plan_output_shape, libdfft), Cint, (Ptr{Cvoid}, Ptr{Int64}), h[], out))
         Plan(h[], Tuple(out))
     end
+end
+
+"One line per kernel launch of a plan (`dfft_plan_describe`)."
+function describe(p::Plan)
+    buf = Vector{UInt8}(undef, 8192)
+    check(ccall((:dfft_plan_describe, libdfft), Cint, (Ptr{Cvoid}, Ptr{UInt8}, Csize_t), p.h, buf, length(buf)))
+    unsafe_string(pointer(buf))
 end
 
 function execute!(p::Plan, out::CuArray, in::CuArray)
