@@ -68,7 +68,7 @@ const GPU_PLAN_CACHE = Dict{Any,Plan}()
 
 function plan_transform(transform, A::CuArray, dims; decomp=Pencil(), n=0, method=0, flags=0)
     dims_t = dims isa Tuple ? dims : (dims,)
-    key = (eltype(A), size(A), typeof(transform), dims_t, decomp, n, method)
+    key = (eltype(A), size(A), typeof(transform), dims_t, decomp, n, method, flags)
     get!(GPU_PLAN_CACHE, key) do
         shape = Int64[size(A)...]
         d = Int32[dims_t...]
