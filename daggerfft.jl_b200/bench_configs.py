@@ -145,7 +145,15 @@ def c4():
 
 
 def c5(rates=(250, 500, 1000, 2000, 4000), seconds=2.0, budget=16 << 30, slots=8):
+    import gc
     import random
+    # plans and buffers of the configurations run before this one are freed
+    # now, not by the garbage collector inside the measured window
+    # (cudaFree waits for the device)
+    gc.collect()
+    dfft.gpu_cleanup_plans()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     edges = [64, 96, 128, 192, 256, 384]
     weights = [30, 20, 20, 15, 10, 5]
     kinds = ["c2c32", "c2c64", "r2c32"]
