@@ -575,10 +575,13 @@ Pass make_pass(const PassSpec& s) {
   if (sp && sp->P > sp->lb) sp = nullptr;
   int variant = s.variant;
   if (variant == VARIANT_AUTO) {
-    // strided axes: the producer-fed kernel unless rows lie 1 MiB or more
-    // apart (each tile then touches L pages, and the narrower tile rows of
-    // that kernel pay the address translation twice as often)
-    if (feed_ok(s, esz) && s.I * (long long)esz < (1LL << 20)) {
+    // strided axes: the producer-fed kernel for passes of 16 MiB and more
+    // (below that its persistent grid is not filled and the one-tile kernels
+    // are as fast), unless rows lie 1 MiB or more apart (each tile then
+    // touches L pages, and the narrower tile rows of that kernel pay the
+    // address translation twice as often)
+    if (feed_ok(s, esz) && s.I * (long long)esz < (1LL << 20) &&
+        (double)s.I * (double)s.O * (double)L * esz >= (double)(16 << 20)) {
       PassSpec t = s;
       t.variant = VARIANT_FEED;
       t.C = 0;

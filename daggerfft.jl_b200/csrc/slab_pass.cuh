@@ -333,6 +333,7 @@ __global__ void __launch_bounds__(LB, MINB)
   static_assert(NC % 32 == 0 && NC + 32 == LB, "whole warps of stage threads plus one producer warp");
   static_assert(NB >= 2 && NB <= 4, "tile buffers");
   constexpr int R0 = first_radix<Rs...>::value;
+  constexpr bool kPow2 = (L & (L - 1)) == 0 && (((Rs & (Rs - 1)) == 0) && ...);
   extern __shared__ __align__(128) unsigned char smem_str[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_str);
   uint64_t* empty = reinterpret_cast<uint64_t*>(smem_str + 32);
@@ -409,9 +410,16 @@ __global__ void __launch_bounds__(LB, MINB)
       if (tile < 0) break;
       V* buf = bufs + b * bst;
       const StrideColC<V, CS> dense{buf + c};
-      const YSwzCol<V, CS, R0> sw{buf + c};
-      static_stages<T, L, P, true, 1, NC, DIR, 1, 1, 0, StrideColC<V, CS>, YSwzCol<V, CS, R0>, StrideColC<V, CS>,
-                    StageTw<V>, Rs...>(d, t, dense, sw, dense, tw, 0, 0, true);
+      if constexpr (kPow2) {
+        // row-swizzled middle stages (bit-split addressing)
+        const YSwzCol<V, CS, R0> sw{buf + c};
+        static_stages<T, L, P, true, 1, NC, DIR, 1, 1, 0, StrideColC<V, CS>, YSwzCol<V, CS, R0>,
+                      StrideColC<V, CS>, StageTw<V>, Rs...>(d, t, dense, sw, dense, tw, 0, 0, true);
+      } else {
+        // other lengths: the plain [row][column] tile (rows of 128 bytes)
+        static_stages<T, L, P, true, 1, NC, DIR, 1, 1, 0, StrideColC<V, CS>, StrideColC<V, CS>,
+                      StrideColC<V, CS>, StageTw<V>, Rs...>(d, t, dense, dense, dense, tw, 0, 0, true);
+      }
       fence_proxy_async_smem();
       stage_sync<NC>();
       if (tid == 0) {

@@ -34,6 +34,21 @@ DFFT_STRIDED_INST(double, 288, 3, 2, 512, 64, 4, 8, 8, 8)
 DFFT_STRIDED_INST(double, 160, 4, 2, 512, 32, 4, 8, 8, 8)
 DFFT_STRIDED_INST(double, 160, 3, 2, 256, 16, 8, 16, 16)
 DFFT_STRIDED_INST(double, 96, 5, 2, 256, 16, 4, 16, 16)
+// lengths of the batched and serving configurations (16 float / 8 double
+// columns: rows of 128 bytes)
+DFFT_STRIDED_INST(float, 128, 8, 2, 48, 6, 16, 6, 8)
+DFFT_STRIDED_INST(float, 160, 6, 2, 64, 8, 16, 8, 8)
+DFFT_STRIDED_INST(float, 160, 6, 2, 80, 8, 16, 10, 8)
+DFFT_STRIDED_INST(float, 160, 6, 2, 96, 8, 16, 12, 8)
+DFFT_STRIDED_INST(float, 192, 5, 2, 120, 10, 16, 12, 10)
+DFFT_STRIDED_INST(float, 192, 4, 2, 160, 10, 16, 10, 16)
+DFFT_STRIDED_INST(float, 224, 4, 2, 192, 12, 16, 12, 16)
+DFFT_STRIDED_INST(float, 416, 2, 2, 384, 48, 8, 6, 8, 8)
+DFFT_STRIDED_INST(double, 96, 6, 2, 64, 8, 8, 8, 8)
+DFFT_STRIDED_INST(double, 96, 5, 2, 96, 8, 8, 12, 8)
+DFFT_STRIDED_INST(double, 96, 6, 2, 128, 8, 8, 16, 8)
+DFFT_STRIDED_INST(double, 128, 3, 2, 192, 12, 8, 12, 16)
+DFFT_STRIDED_INST(double, 416, 1, 2, 384, 48, 8, 6, 8, 8)
 
 static const SlabKernel kStridedKernels[] = {
     // dbl, L, P, nst, radices, threads, CS, NB, dflt, forward and inverse kernels
@@ -50,6 +65,19 @@ static const SlabKernel kStridedKernels[] = {
     {1, 512, 32, 3, {8, 8, 8}, 160, 4, 2, 1, K(double, 160, 4, 2, 512, 32, 4, 8, 8, 8)},
     {1, 256, 16, 2, {16, 16}, 160, 8, 2, 1, K(double, 160, 3, 2, 256, 16, 8, 16, 16)},
     {1, 256, 16, 2, {16, 16}, 96, 4, 2, 1, K(double, 96, 5, 2, 256, 16, 4, 16, 16)},
+    {0, 48, 6, 2, {6, 8}, 128, 16, 2, 1, K(float, 128, 8, 2, 48, 6, 16, 6, 8)},
+    {0, 64, 8, 2, {8, 8}, 160, 16, 2, 1, K(float, 160, 6, 2, 64, 8, 16, 8, 8)},
+    {0, 80, 8, 2, {10, 8}, 160, 16, 2, 1, K(float, 160, 6, 2, 80, 8, 16, 10, 8)},
+    {0, 96, 8, 2, {12, 8}, 160, 16, 2, 1, K(float, 160, 6, 2, 96, 8, 16, 12, 8)},
+    {0, 120, 10, 2, {12, 10}, 192, 16, 2, 1, K(float, 192, 5, 2, 120, 10, 16, 12, 10)},
+    {0, 160, 10, 2, {10, 16}, 192, 16, 2, 1, K(float, 192, 4, 2, 160, 10, 16, 10, 16)},
+    {0, 192, 12, 2, {12, 16}, 224, 16, 2, 1, K(float, 224, 4, 2, 192, 12, 16, 12, 16)},
+    {0, 384, 48, 3, {6, 8, 8}, 416, 8, 2, 1, K(float, 416, 2, 2, 384, 48, 8, 6, 8, 8)},
+    {1, 64, 8, 2, {8, 8}, 96, 8, 2, 1, K(double, 96, 6, 2, 64, 8, 8, 8, 8)},
+    {1, 96, 8, 2, {12, 8}, 96, 8, 2, 1, K(double, 96, 5, 2, 96, 8, 8, 12, 8)},
+    {1, 128, 8, 2, {16, 8}, 96, 8, 2, 1, K(double, 96, 6, 2, 128, 8, 8, 16, 8)},
+    {1, 192, 12, 2, {12, 16}, 128, 8, 2, 1, K(double, 128, 3, 2, 192, 12, 8, 12, 16)},
+    {1, 384, 48, 3, {6, 8, 8}, 416, 8, 2, 1, K(double, 416, 1, 2, 384, 48, 8, 6, 8, 8)},
 };
 
 #undef K

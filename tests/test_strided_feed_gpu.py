@@ -15,7 +15,16 @@ pytestmark = pytest.mark.gpu
 CASES = [((64, 512, 12), 2, np.complex64, 4), ((72, 512, 6), 2, np.complex64, 4),
          ((16, 8, 512), 3, np.complex64, 4), ((40, 256, 20), 2, np.complex64, 3),
          ((128, 128, 30), 2, np.complex64, 2), ((24, 512, 6), 2, np.complex128, 2),
-         ((32, 256, 18), 2, np.complex128, 2)]
+         ((32, 256, 18), 2, np.complex128, 2),
+         # lengths of the batched / serving configurations (plain row layout
+         # unless a power of two)
+         ((32, 48, 6), 2, np.complex64, 1), ((16, 64, 8), 2, np.complex64, 1),
+         ((32, 80, 6), 2, np.complex64, 1), ((16, 8, 96), 3, np.complex64, 1),
+         ((48, 120, 4), 2, np.complex64, 1), ((16, 160, 4), 2, np.complex64, 1),
+         ((32, 192, 4), 2, np.complex64, 1), ((16, 384, 2), 2, np.complex64, 1),
+         ((16, 64, 8), 2, np.complex128, 1), ((8, 96, 8), 2, np.complex128, 1),
+         ((8, 128, 4), 2, np.complex128, 1), ((8, 192, 4), 2, np.complex128, 1),
+         ((8, 384, 2), 2, np.complex128, 1)]
 
 
 def _forced_plan(tag, g, dim, idx, tmp_path):
