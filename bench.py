@@ -191,6 +191,16 @@ def run_profile(args):
     B = dfft.empty_like_layout(A.shape, A.dtype, A)
     dims = tuple(int(c) for c in args.profile)
     flags = (0 if args.no_tune else dfft.FLAG_TUNE) | (dfft.FLAG_NO_FUSE if args.no_fuse else 0)
+    if args.slab_variant >= 0:
+        # pin the fused slab kernel's variant through a one-line wisdom file
+        # (key: device name with blanks as '_', '_sm' + SM count, 'slab',
+        # double?, L, O, inverse), so no tuning launches precede the profiled ones
+        prop = torch.cuda.get_device_properties(0)
+        tag = prop.name.replace(" ", "_").replace("|", "_") + f"_sm{prop.multi_processor_count}"
+        with tempfile.NamedTemporaryFile("w", suffix=".wisdom", delete=False) as f:
+            f.write(f"{tag}|slab|0|{shape[0]}|{shape[2]}|0 {args.slab_variant} 0 0\n")
+        dfft.wisdom_import(f.name)
+        os.unlink(f.name)
     p = dfft.gpu_plan_transform(dfft.FFT(), A, dims, method=args.method, flags=flags)
     for _ in range(2):
         p.execute(A, B)
@@ -213,6 +223,8 @@ def main():
     ap.add_argument("--no-fuse", action="store_true",
                     help="one pass per axis (no fused dims-(1,2) slab pass)")
     ap.add_argument("--shape", default="512,512,512", help="profiling mode: ComplexF32 array shape")
+    ap.add_argument("--slab-variant", type=int, default=-1,
+                    help="profiling mode: the fused slab kernel's variant (index into its table)")
     args = ap.parse_args()
     if args.profile:
         run_profile(args)

@@ -81,9 +81,12 @@ int dfft_plan_describe(dfft_plan plan, char* buf, size_t len) {
                          : q.tiled == 1 ? "tiled-contig" : q.tiled == 2 ? "tiled-strided"
                          : q.pipe ? (q.tma ? "strided-pipe" : "contig-pipe")
                          : q.is_static ? "direct" : "dynamic";
+      std::string rad;
+      for (int i = 0; i < q.d.nst; ++i) rad += (i ? "x" : "") + std::to_string(q.d.radix[i]);
       char line[256];
-      std::snprintf(line, sizeof line, "%s L=%d I=%lld O=%lld grid=%u block=%u smem=%zu\n", kind, q.d.L,
-                    q.d.I, q.d.I > 0 ? q.d.Q / q.d.I : 0LL, q.grid.x, q.block.x, q.smem);
+      std::snprintf(line, sizeof line, "%s L=%d I=%lld O=%lld grid=%u block=%u smem=%zu radices=%s\n", kind,
+                    q.d.L, q.d.I, q.d.I > 0 ? q.d.Q / q.d.I : 0LL, q.grid.x, q.block.x, q.smem,
+                    rad.empty() ? "-" : rad.c_str());
       out += line;
     }
     const size_t n = out.size() < len - 1 ? out.size() : len - 1;

@@ -582,12 +582,17 @@ Pass make_pass(const PassSpec& s) {
     // address translation twice as often)
     if (feed_ok(s, esz) && s.I * (long long)esz < (1LL << 20) &&
         (double)s.I * (double)s.O * (double)L * esz >= (double)(16 << 20)) {
-      PassSpec t = s;
-      t.variant = VARIANT_FEED;
-      t.C = 0;
-      try {
-        return make_pass(t);
-      } catch (const Error&) {
+      // the first (fastest) default launch shape whose tile width fits I
+      for (int v = 0; const SlabKernel* k = find_strided_kernel(s.dbl, L, v); ++v) {
+        if (!k->dflt || k->cs > s.I) continue;
+        PassSpec t = s;
+        t.variant = VARIANT_FEED;
+        t.C = v;
+        try {
+          return make_pass(t);
+        } catch (const Error&) {
+        }
+        break;
       }
     }
     if (pipe_strided_ok(s, sp, esz) || pipe_contig_ok(s, sp, esz)) {

@@ -14,7 +14,8 @@
 // Persistent CTAs of C*P stage threads plus one producer warp.  A tile is C
 // consecutive pencils: its input and its output are each one contiguous run
 // (C*M or C*(M+1) complex elements), moved by one 1-D bulk copy into / out
-// of an NB-deep ring of tile buffers.  R2C: the stages read the dense tile
+// of an NB-deep ring of tile buffers; the producer issues both copies (the
+// store when the stage threads hand the buffer back, before refilling it).  R2C: the stages read the dense tile
 // and run in a padded work buffer; the post-pass writes the M+1 outputs of
 // each pencil back into the (consumed) tile buffer.  C2R: the pre-pass reads
 // the tile and writes the work buffer; the stages end in the tile buffer.
@@ -81,13 +82,28 @@ __global__ void __launch_bounds__(LB, MINB) real_pass(const PassDesc d, const Re
     if (tid == NC) {
       // ---------------- producer ----------------
       const uint32_t in_bytes = (uint32_t)((size_t)C * IN_E * sizeof(V));
+      const uint32_t out_bytes = (uint32_t)((size_t)C * OUT_E * sizeof(V));
       const V* src = reinterpret_cast<const V*>(d.in.p);
+      V* dst = reinterpret_cast<V*>(d.out.p);
       int fills[NB] = {};
+      long long pend[NB];  // transformed tile in buffer b still to be stored, or -1
+      for (int bb = 0; bb < NB; ++bb) pend[bb] = -1;
       bool failed = false;
+      // waits until the stage threads hand buffer b back, then stores its
+      // tile and waits until the store has read the buffer
+      auto drain = [&](int b) -> bool {
+        if (pend[b] < 0) return true;
+        if (!mbar_wait_bounded(&empty[b], (uint32_t)((fills[b] - 1) & 1))) return false;
+        bulk_store_1d(dst + pend[b] * C * OUT_E, bufs + b * bst, out_bytes);
+        bulk_commit();
+        bulk_wait_read_all();
+        pend[b] = -1;
+        return true;
+      };
       long long tile = blockIdx.x;
       for (int it = 0;; ++it) {
         const int b = it % NB;
-        if (fills[b] > 0 && !mbar_wait_bounded(&empty[b], (uint32_t)((fills[b] - 1) & 1))) {
+        if (!drain(b)) {
           failed = true;
           break;
         }
@@ -100,9 +116,13 @@ __global__ void __launch_bounds__(LB, MINB) real_pass(const PassDesc d, const Re
         }
         mbar_expect_tx(&full[b], in_bytes);
         bulk_load_1d(bufs + b * bst, src + tile * C * IN_E, in_bytes, &full[b]);
+        pend[b] = tile;
         tile += gridDim.x;
       }
+      for (int bb = 0; bb < NB && !failed; ++bb)
+        if (!drain(bb)) failed = true;
       if (failed && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
+      bulk_wait_all();
       for (int bb = 0; bb < NB; ++bb)
         if (fills[bb] > 0) mbar_wait_bounded(&full[bb], (uint32_t)((fills[bb] - 1) & 1));
     }
@@ -111,8 +131,6 @@ __global__ void __launch_bounds__(LB, MINB) real_pass(const PassDesc d, const Re
     const StageTw<V> tw{stw};
     const int t = tid % P, c = tid / P;
     const PadCol<V> pad{work + (size_t)c * g.ld};
-    const uint32_t out_bytes = (uint32_t)((size_t)C * OUT_E * sizeof(V));
-    V* dst = reinterpret_cast<V*>(d.out.p);
     for (int it = 0;; ++it) {
       const int b = it % NB;
       if (!mbar_wait_bounded(&full[b], (uint32_t)((it / NB) & 1))) s_cabort = 1;
@@ -151,19 +169,11 @@ __global__ void __launch_bounds__(LB, MINB) real_pass(const PassDesc d, const Re
         static_stages<T, M, P, true, 1, NC, 2, 1, 1, 0, PadCol<V>, PadCol<V>, StrideCol<V>, StageTw<V>, Rs...>(
             d, t, pad, pad, dense, tw, 0, 0, true);
       }
-      fence_proxy_async_smem();
+      fence_proxy_async_smem();  // the producer's bulk store reads the tile next
       stage_sync<NC>();
-      if (tid == 0) {
-        bulk_store_1d(dst + tile * C * OUT_E, buf, out_bytes);
-        bulk_commit();
-        bulk_wait_read_all();  // the store has read the tile: the buffer goes back
-        mbar_arrive(&empty[b]);
-      }
+      if (tid == 0) mbar_arrive(&empty[b]);  // hand the transformed tile to the producer
     }
-    if (tid == 0) {
-      bulk_wait_all();
-      if (s_cabort && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
-    }
+    if (tid == 0 && s_cabort && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
   }
   __syncthreads();
 }

@@ -25,6 +25,8 @@ DFFT_SLAB_INST(float, 160, 6, 2, 512, 32, 4, 8, 8, 8)
 DFFT_SLAB_INST(float, 288, 4, 2, 512, 64, 4, 8, 8, 8)
 DFFT_SLAB_INST(float, 160, 4, 3, 512, 32, 4, 8, 8, 8)
 DFFT_SLAB_INST(float, 288, 2, 3, 512, 32, 8, 8, 8, 8)
+// ComplexF32, L = 512 (32 x 16): one exchange per axis, 32 elements per thread
+DFFT_SLAB_INST(float, 160, 3, 2, 512, 16, 8, 32, 16)
 // ComplexF32, L = 256 (16 x 16) and 128 (16 x 8)
 DFFT_SLAB_INST(float, 160, 5, 2, 256, 16, 8, 16, 16)
 DFFT_SLAB_INST(float, 160, 6, 2, 256, 16, 8, 16, 16)
@@ -46,6 +48,7 @@ DFFT_SLAB_INST(double, 96, 3, 3, 256, 16, 4, 16, 16)
 // DFFT_FLAG_FUSE selects the fused kernel there).
 static const SlabKernel kSlabKernels[] = {
     // dbl, L, P, nst, radices, threads, CS, NB, dflt, forward and inverse kernels
+    {0, 512, 16, 2, {32, 16}, 160, 8, 2, 1, K(float, 160, 3, 2, 512, 16, 8, 32, 16)},
     {0, 512, 32, 3, {8, 8, 8}, 160, 4, 2, 1, K(float, 160, 6, 2, 512, 32, 4, 8, 8, 8)},
     {0, 512, 32, 3, {8, 8, 8}, 160, 4, 2, 1, K(float, 160, 5, 2, 512, 32, 4, 8, 8, 8)},
     {0, 512, 32, 3, {8, 8, 8}, 160, 4, 3, 1, K(float, 160, 4, 3, 512, 32, 4, 8, 8, 8)},

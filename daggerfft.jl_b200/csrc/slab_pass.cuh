@@ -20,9 +20,11 @@
 // counter, works through them in order, waits
 // until a y-job's slab has all its x-tiles, issues the tile loads into
 // NB buffers (full barriers), and, when the stage threads hand a buffer
-// back (empty barriers), publishes a finished x-tile in the slab's counter.
-// The stage threads synchronise on named barrier 1 only, so no global atomic
-// or counter wait sits on their path.
+// back (empty barriers), publishes a finished x-tile in the slab's counter
+// or issues the TMA store of a finished y-tile (and waits until the store
+// has read the buffer before refilling it).  The stage threads synchronise
+// on named barrier 1 only, so no global atomic, counter wait or store wait
+// sits on their path.
 //
 // Progress: x-jobs never wait on other jobs, a CTA works through its claimed
 // jobs in claim order, and a producer publishes its own finished x-tiles
@@ -173,13 +175,22 @@ __global__ void __launch_bounds__(LB, MINB)
       int fills[NB] = {};  // arrivals on full[b]
       int kindb[NB] = {};  // job in buffer b not yet handed back
       int slabb[NB] = {};
+      int tileb[NB] = {};
       bool failed = false;
-      // waits until the stage threads hand buffer b back; publishes an x-tile
+      // waits until the stage threads hand buffer b back; publishes an
+      // x-tile, or stores a y-tile and waits until the store has read it
       auto settle = [&](int b) -> bool {
         if (kindb[b] == 0) return true;
         if (!mbar_wait_bounded(&empty[b], (uint32_t)((fills[b] - 1) & 1))) return false;
-        if (kindb[b] == 1)  // release: the stage threads' stores, seen through the barrier, first
+        if (kindb[b] == 1) {  // release: the stage threads' stores, seen through the barrier, first
           asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(g.done + slabb[b]) : "memory");
+        } else {
+          const V* buf = bufs + b * bst;
+          for (int kb = 0; kb < g.nlb; ++kb)
+            tma_store_3d(&tout, buf + (size_t)kb * g.lb * CS, tileb[b] * CS * g.xscale, kb * g.lb, slabb[b]);
+          bulk_commit();
+          bulk_wait_read_all();
+        }
         kindb[b] = 0;
         return true;
       };
@@ -244,11 +255,14 @@ __global__ void __launch_bounds__(LB, MINB)
         }
         kindb[b] = J.kind;
         slabb[b] = J.slab;
+        tileb[b] = J.tile;
       }
-      // publish the x-tiles still held by this CTA
+      // publish the x-tiles and store the y-tiles still held by this CTA
+      // (on the error path too: other CTAs may wait for these x-tiles)
       for (int bb = 0; bb < NB; ++bb)
         if (!settle(bb)) failed = true;
       if (failed && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
+      bulk_wait_all();
       // no bulk copy may still be landing in shared memory when the CTA exits
       for (int bb = 0; bb < NB; ++bb)
         if (fills[bb] > 0) mbar_wait_bounded(&full[bb], (uint32_t)((fills[bb] - 1) & 1));
@@ -283,20 +297,9 @@ __global__ void __launch_bounds__(LB, MINB)
       }
       fence_proxy_async_smem();  // the buffer is next read (store) or written (load) by TMA
       stage_sync<NC>();
-      if (tid == 0) {
-        if (J.kind == 2) {
-          for (int kb = 0; kb < g.nlb; ++kb)
-            tma_store_3d(&tout, buf + (size_t)kb * g.lb * CS, J.tile * CS * g.xscale, kb * g.lb, J.slab);
-          bulk_commit();
-          bulk_wait_read_all();  // the store has read the tile: the buffer goes back
-        }
-        mbar_arrive(&empty[b]);
-      }
+      if (tid == 0) mbar_arrive(&empty[b]);  // the producer publishes (x) or stores (y) the tile
     }
-    if (tid == 0) {
-      bulk_wait_all();
-      if (s_cabort && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
-    }
+    if (tid == 0 && s_cabort && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
   }
   __syncthreads();
 }
@@ -311,7 +314,8 @@ namespace dfft {
 // is CS columns x L rows (x = (t % tiles_i)*CS, z = t / tiles_i), loaded
 // and stored by TMA boxes {CS*xscale, lb, 1}; CTA b takes tiles b, b+grid, ...
 // The producer (lane 0 of the last warp) fills NB buffers as the stage
-// threads hand them back; the stage threads run the stages in the
+// threads hand them back, storing each transformed tile (TMA) before it
+// refills the buffer; the stage threads run the stages in the
 // row-swizzled layout with the stage twiddles in shared memory and sync on
 // named barrier 1.  Bounded waits as in the slab pass.
 // ---------------------------------------------------------------------------
@@ -368,12 +372,29 @@ __global__ void __launch_bounds__(LB, MINB)
       // ---------------- producer ----------------
       const uint32_t tile_bytes = (uint32_t)((size_t)CS * L * sizeof(V));
       int fills[NB] = {};
+      long long pend[NB];  // transformed tile in buffer b still to be stored, or -1
+      for (int bb = 0; bb < NB; ++bb) pend[bb] = -1;
       bool failed = false;
+      // waits until the stage threads hand buffer b back, then stores its
+      // tile and waits until the store has read the buffer
+      auto drain = [&](int b) -> bool {
+        if (pend[b] < 0) return true;
+        if (!mbar_wait_bounded(&empty[b], (uint32_t)((fills[b] - 1) & 1))) return false;
+        const int ti = (int)(pend[b] % g.tiles_i);
+        const int o = (int)(pend[b] / g.tiles_i);
+        const V* buf = bufs + b * bst;
+        for (int kb = 0; kb < g.nlb; ++kb)
+          tma_store_3d(&tout, buf + (size_t)kb * g.lb * CS, ti * CS * g.xscale, kb * g.lb, o);
+        bulk_commit();
+        bulk_wait_read_all();
+        pend[b] = -1;
+        return true;
+      };
       long long tile = blockIdx.x;
       for (int it = 0;; ++it) {
         const int b = it % NB;
-        // the buffer's previous tile must be handed back first
-        if (fills[b] > 0 && !mbar_wait_bounded(&empty[b], (uint32_t)((fills[b] - 1) & 1))) {
+        // the buffer's previous tile must be handed back and stored first
+        if (!drain(b)) {
           failed = true;
           break;
         }
@@ -390,9 +411,14 @@ __global__ void __launch_bounds__(LB, MINB)
         mbar_expect_tx(&full[b], tile_bytes);
         for (int kb = 0; kb < g.nlb; ++kb)
           tma_load_3d(buf + (size_t)kb * g.lb * CS, &tin, &full[b], ti * CS * g.xscale, kb * g.lb, o);
+        pend[b] = tile;
         tile += gridDim.x;
       }
+      // the tiles the stage threads still hold
+      for (int bb = 0; bb < NB && !failed; ++bb)
+        if (!drain(bb)) failed = true;
       if (failed && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
+      bulk_wait_all();
       // no bulk copy may still be landing in shared memory when the CTA exits
       for (int bb = 0; bb < NB; ++bb)
         if (fills[bb] > 0) mbar_wait_bounded(&full[bb], (uint32_t)((fills[bb] - 1) & 1));
@@ -420,22 +446,11 @@ __global__ void __launch_bounds__(LB, MINB)
         static_stages<T, L, P, true, 1, NC, DIR, 1, 1, 0, StrideColC<V, CS>, StrideColC<V, CS>,
                       StrideColC<V, CS>, StageTw<V>, Rs...>(d, t, dense, dense, dense, tw, 0, 0, true);
       }
-      fence_proxy_async_smem();
+      fence_proxy_async_smem();  // the producer's TMA store reads the tile next
       stage_sync<NC>();
-      if (tid == 0) {
-        const int ti = (int)(tile % g.tiles_i);
-        const int o = (int)(tile / g.tiles_i);
-        for (int kb = 0; kb < g.nlb; ++kb)
-          tma_store_3d(&tout, buf + (size_t)kb * g.lb * CS, ti * CS * g.xscale, kb * g.lb, o);
-        bulk_commit();
-        bulk_wait_read_all();  // the store has read the tile: the buffer goes back
-        mbar_arrive(&empty[b]);
-      }
+      if (tid == 0) mbar_arrive(&empty[b]);  // hand the transformed tile to the producer
     }
-    if (tid == 0) {
-      bulk_wait_all();
-      if (s_cabort && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
-    }
+    if (tid == 0 && s_cabort && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
   }
   __syncthreads();
 }

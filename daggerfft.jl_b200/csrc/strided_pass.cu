@@ -23,6 +23,10 @@ DFFT_STRIDED_INST(float, 288, 3, 2, 512, 32, 8, 8, 8, 8)
 DFFT_STRIDED_INST(float, 288, 2, 3, 512, 32, 8, 8, 8, 8)
 DFFT_STRIDED_INST(float, 160, 6, 2, 512, 32, 4, 8, 8, 8)
 DFFT_STRIDED_INST(float, 544, 1, 2, 512, 32, 16, 8, 8, 8)
+// ComplexF32, L = 512 (32 x 16): one exchange, 32 elements per thread
+DFFT_STRIDED_INST(float, 288, 1, 2, 512, 16, 16, 32, 16)
+DFFT_STRIDED_INST(float, 288, 1, 3, 512, 16, 16, 32, 16)
+DFFT_STRIDED_INST(float, 160, 3, 2, 512, 16, 8, 32, 16)
 // ComplexF32, L = 256 (16 x 16) and 128 (16 x 8)
 DFFT_STRIDED_INST(float, 288, 3, 2, 256, 16, 16, 16, 16)
 DFFT_STRIDED_INST(float, 288, 2, 3, 256, 16, 16, 16, 16)
@@ -52,10 +56,13 @@ DFFT_STRIDED_INST(double, 416, 1, 2, 384, 48, 8, 6, 8, 8)
 
 static const SlabKernel kStridedKernels[] = {
     // dbl, L, P, nst, radices, threads, CS, NB, dflt, forward and inverse kernels
+    {0, 512, 16, 2, {32, 16}, 288, 16, 2, 1, K(float, 288, 1, 2, 512, 16, 16, 32, 16)},
     {0, 512, 32, 3, {8, 8, 8}, 288, 8, 3, 1, K(float, 288, 2, 3, 512, 32, 8, 8, 8, 8)},
     {0, 512, 32, 3, {8, 8, 8}, 288, 8, 2, 1, K(float, 288, 3, 2, 512, 32, 8, 8, 8, 8)},
     {0, 512, 32, 3, {8, 8, 8}, 160, 4, 2, 1, K(float, 160, 6, 2, 512, 32, 4, 8, 8, 8)},
     {0, 512, 32, 3, {8, 8, 8}, 544, 16, 2, 1, K(float, 544, 1, 2, 512, 32, 16, 8, 8, 8)},
+    {0, 512, 16, 2, {32, 16}, 288, 16, 3, 1, K(float, 288, 1, 3, 512, 16, 16, 32, 16)},
+    {0, 512, 16, 2, {32, 16}, 160, 8, 2, 1, K(float, 160, 3, 2, 512, 16, 8, 32, 16)},
     {0, 256, 16, 2, {16, 16}, 288, 16, 2, 1, K(float, 288, 3, 2, 256, 16, 16, 16, 16)},
     {0, 256, 16, 2, {16, 16}, 288, 16, 3, 1, K(float, 288, 2, 3, 256, 16, 16, 16, 16)},
     {0, 256, 16, 2, {16, 16}, 160, 8, 2, 1, K(float, 160, 6, 2, 256, 16, 8, 16, 16)},

@@ -8,7 +8,7 @@
 // and writing the tile, compiled in for the kind (r2r_load / r2r_store);
 // every read of a tile precedes the first stage's barrier, so the output
 // overwrites the input in place, and the tile leaves by the same kind of
-// copy.  The FFT runs in a padded complex work buffer, one column per C.
+// copy, which the producer issues when the buffer is handed back.  The FFT runs in a padded complex work buffer, one column per C.
 // Bounded waits as in the other pipelined passes.
 #pragma once
 #include "real_pass.cuh"
@@ -84,12 +84,34 @@ __global__ void __launch_bounds__(LB, MINB)
     if (tid == NC) {
       // ---------------- producer ----------------
       const uint32_t in_bytes = (uint32_t)((size_t)C * g.n_in * sizeof(T));
+      const uint32_t out_bytes = (uint32_t)((size_t)C * g.n_out * sizeof(T));
       int fills[NB] = {};
+      long long pend[NB];  // transformed tile in buffer b still to be stored, or -1
+      for (int bb = 0; bb < NB; ++bb) pend[bb] = -1;
       bool failed = false;
+      // waits until the stage threads hand buffer b back, then stores its
+      // tile and waits until the store has read the buffer
+      auto drain = [&](int b) -> bool {
+        if (pend[b] < 0) return true;
+        if (!mbar_wait_bounded(&empty[b], (uint32_t)((fills[b] - 1) & 1))) return false;
+        unsigned char* buf = bufs + b * bst;
+        if (STRIDED) {
+          const int ti = (int)(pend[b] % g.tiles_i);
+          const int o = (int)(pend[b] / g.tiles_i);
+          for (int kb = 0; kb < g.nlb; ++kb)
+            tma_store_3d(&tout, buf + (size_t)kb * g.lb * C * sizeof(T), ti * C, kb * g.lb, o);
+        } else {
+          bulk_store_1d(reinterpret_cast<T*>(g.dst) + pend[b] * C * g.n_out, buf, out_bytes);
+        }
+        bulk_commit();
+        bulk_wait_read_all();
+        pend[b] = -1;
+        return true;
+      };
       long long tile = blockIdx.x;
       for (int it = 0;; ++it) {
         const int b = it % NB;
-        if (fills[b] > 0 && !mbar_wait_bounded(&empty[b], (uint32_t)((fills[b] - 1) & 1))) {
+        if (!drain(b)) {
           failed = true;
           break;
         }
@@ -110,9 +132,13 @@ __global__ void __launch_bounds__(LB, MINB)
         } else {
           bulk_load_1d(buf, reinterpret_cast<const T*>(g.src) + tile * C * g.n_in, in_bytes, &full[b]);
         }
+        pend[b] = tile;
         tile += gridDim.x;
       }
+      for (int bb = 0; bb < NB && !failed; ++bb)
+        if (!drain(bb)) failed = true;
       if (failed && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
+      bulk_wait_all();
       for (int bb = 0; bb < NB; ++bb)
         if (fills[bb] > 0) mbar_wait_bounded(&full[bb], (uint32_t)((fills[bb] - 1) & 1));
     }
@@ -132,7 +158,6 @@ __global__ void __launch_bounds__(LB, MINB)
     const size_t ob = STRIDED ? c : (size_t)c * g.n_out;
     const V* w_in = reinterpret_cast<const V*>(d.in.w);
     const V* w_out = reinterpret_cast<const V*>(d.out.w);
-    const uint32_t out_bytes = (uint32_t)((size_t)C * g.n_out * sizeof(T));
     for (int it = 0;; ++it) {
       const int b = it % NB;
       if (!mbar_wait_bounded(&full[b], (uint32_t)((it / NB) & 1))) s_cabort = 1;
@@ -145,26 +170,11 @@ __global__ void __launch_bounds__(LB, MINB)
       const Out out{reinterpret_cast<T*>(buf) + ob, d.out.n, w_out};
       static_stages<T, L, P, true, 1, NC, DIR, 1, 1, 0, In, PadCol<V>, Out, GlobalTw<V>, Rs...>(d, t, in, col, out,
                                                                                             tw, 0, 0, true);
-      fence_proxy_async_smem();
+      fence_proxy_async_smem();  // the producer's store reads the tile next
       stage_sync<NC>();
-      if (tid == 0) {
-        if (STRIDED) {
-          const int ti = (int)(tile % g.tiles_i);
-          const int o = (int)(tile / g.tiles_i);
-          for (int kb = 0; kb < g.nlb; ++kb)
-            tma_store_3d(&tout, buf + (size_t)kb * g.lb * C * sizeof(T), ti * C, kb * g.lb, o);
-        } else {
-          bulk_store_1d(reinterpret_cast<T*>(g.dst) + tile * C * g.n_out, buf, out_bytes);
-        }
-        bulk_commit();
-        bulk_wait_read_all();
-        mbar_arrive(&empty[b]);
-      }
+      if (tid == 0) mbar_arrive(&empty[b]);  // hand the transformed tile to the producer
     }
-    if (tid == 0) {
-      bulk_wait_all();
-      if (s_cabort && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
-    }
+    if (tid == 0 && s_cabort && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
   }
   __syncthreads();
 }

@@ -125,7 +125,7 @@ DFFT_API int dfft_plan_workspace_bytes(dfft_plan plan, size_t* bytes);
 DFFT_API int dfft_plan_launches(dfft_plan plan, int* launches);
 
 /* One line per kernel launch of the plan ("<kernel> L=.. I=.. O=.. grid=..
- * block=.. smem=.."), NUL-terminated and truncated to len-1 characters
+ * block=.. smem=.. radices=AxBx.."), NUL-terminated and truncated to len-1 characters
  * (the analogue of fftw_sprint_plan; for logs and tests). */
 DFFT_API int dfft_plan_describe(dfft_plan plan, char* buf, size_t len);
 

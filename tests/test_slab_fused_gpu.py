@@ -132,3 +132,46 @@ def test_untuned_default_per_length():
         p = _plan(dfft.FFT(), g, (1, 2), flags=0)
         assert p.launches == (1 if fused else 2)
         assert rel(to_np(_run(p, g)), oracle.fft(a, dims=(1, 2))) <= 1e-5
+
+
+# fused variants per (dtype, L), the order of the kernel table
+N_VARIANTS = {(np.complex64, 512): 6, (np.complex64, 256): 4, (np.complex64, 128): 2,
+              (np.complex128, 512): 3, (np.complex128, 256): 3}
+
+
+def _forced_slab_plan(tag, g, v, tmp_path):
+    # tune once to learn the slab wisdom key, then force variant v through
+    # an edited wisdom file
+    dfft.wisdom_forget()
+    dfft.gpu_plan_transform(tag, g, (1, 2), decomp=dfft.Slab(), flags=dfft.FLAG_TUNE)
+    f = tmp_path / "w.txt"
+    dfft.wisdom_export(f)
+    keys = [ln.split()[0] for ln in f.read_text().splitlines() if "|slab|" in ln]
+    assert len(keys) == 1
+    f.write_text(f"{keys[0]} {v} 0 0\n")
+    dfft.wisdom_forget()
+    dfft.wisdom_import(f)
+    p = dfft.gpu_plan_transform(tag, g, (1, 2), decomp=dfft.Slab())
+    dfft.wisdom_forget()
+    return p
+
+
+@pytest.mark.parametrize("dtype,L", list(N_VARIANTS))
+@pytest.mark.parametrize("inverse", [False, True])
+def test_every_fused_variant(dtype, L, inverse, tmp_path):
+    O = 6
+    a = rand((L, L, O), dtype, seed=L + 7 * inverse)
+    g = to_gpu(a)
+    tag = dfft.IFFT() if inverse else dfft.FFT()
+    ref = (oracle.ifft if inverse else oracle.fft)(a, dims=(1, 2))
+    radices = set()
+    for v in range(N_VARIANTS[(dtype, L)]):
+        p = _forced_slab_plan(tag, g, v, tmp_path)
+        d = p.describe().strip()
+        assert p.launches == 1 and d.startswith("slab-xy"), d
+        radices.add(d.split("radices=")[1])
+        y = _run(p, g)
+        assert dfft.device_error() == 0
+        assert rel(to_np(y), ref) <= tol_for(dtype), (v, d)
+    if (dtype, L) == (np.complex64, 512):
+        assert radices == {"8x8x8", "32x16"}

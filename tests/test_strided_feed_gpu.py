@@ -12,8 +12,8 @@ from helpers import rand, rel, to_gpu, to_np, tol_for
 pytestmark = pytest.mark.gpu
 
 # (shape, dim, dtype, launch shapes of that length)
-CASES = [((64, 512, 12), 2, np.complex64, 4), ((72, 512, 6), 2, np.complex64, 4),
-         ((16, 8, 512), 3, np.complex64, 4), ((40, 256, 20), 2, np.complex64, 3),
+CASES = [((64, 512, 12), 2, np.complex64, 7), ((72, 512, 6), 2, np.complex64, 7),
+         ((16, 8, 512), 3, np.complex64, 7), ((40, 256, 20), 2, np.complex64, 3),
          ((128, 128, 30), 2, np.complex64, 2), ((24, 512, 6), 2, np.complex128, 2),
          ((32, 256, 18), 2, np.complex128, 2),
          # lengths of the batched / serving configurations (plain row layout
@@ -63,7 +63,8 @@ def test_in_place_and_c_order(tmp_path):
     a = rand((48, 512, 8), np.complex64, seed=5)
     for order in ["F", "C"]:
         g = to_gpu(a, order)
-        p = _forced_plan(dfft.FFT(), g, 2, 0, tmp_path)
+        # launch shape 1 (8-column tiles) fits both layouts: I = 48 (F), 8 (C)
+        p = _forced_plan(dfft.FFT(), g, 2, 1, tmp_path)
         assert "strided-feed" in p.describe()
         p.execute(g, g)
         assert rel(to_np(g), oracle.fft(a, dims=(2,))) <= 1e-5
@@ -75,3 +76,16 @@ def test_describe_lists_every_launch():
     d = p.describe().strip().splitlines()
     assert len(d) == p.launches
     assert d[0].startswith("slab-xy L=256")
+
+
+def test_untuned_shape_fits_the_columns():
+    # untuned plans take the first launch shape whose tile is not wider than
+    # the columns along the contiguous axes (16-column tiles need I >= 16)
+    for shape in [(8, 512, 1100), (64, 512, 140)]:
+        a = rand(shape, np.complex64, seed=shape[0])
+        g = to_gpu(a)
+        p = dfft.gpu_plan_transform(dfft.FFT(), g, (2,))
+        assert "strided-feed" in p.describe(), p.describe()
+        out = dfft.empty_like_layout(p.out_shape, g.dtype, g)
+        p.execute(g, out)
+        assert rel(to_np(out), oracle.fft(a, dims=(2,))) <= 1e-5
