@@ -370,7 +370,8 @@ template <int BAR> __device__ __forceinline__ void stage_sync() {
 // exactly ceil((L/R)/P), in the dynamic kernel EMAX/R.
 // SMEM_IO: 0 = the first stage reads and the last stage writes global
 // memory; 1 = both go through shared memory (pipelined kernels); 2 = the
-// first stage reads shared memory, the last stage writes global memory.
+// first stage reads shared memory, the last stage writes whole pencils to
+// global memory (unit stride); 3 = the same with the output's row stride.
 // CIN/COUT: the shared-memory views the stage reads and writes (they differ
 // when a stage moves a tile between a dense TMA buffer and a padded one).
 // toff: offset of this stage in a StageTw table (Ns - R_0).
@@ -429,7 +430,8 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
           if (cv) {
             V y = v[b][r];
             if (inv) y.y = -y.y;
-            // SMEM_IO 2 (the fused slab pass) stores whole pencils: unit stride
+            // SMEM_IO 2 (the fused slab pass) stores whole pencils: unit stride;
+            // SMEM_IO 3 (the cp.async strided pass) rows d.out.sk apart
             if (FAST_IO) reinterpret_cast<V*>(d.out.p)[ob + (SMEM_IO == 2 ? k : k * d.out.sk)] = cscale(y, scale);
             else store_elem<T>(d.out, ob, k, y, scale);
           }

@@ -77,7 +77,8 @@ int dfft_plan_describe(dfft_plan plan, char* buf, size_t len) {
     if (!buf || len == 0) throw Error{DFFT_ERROR_INVALID_VALUE, "buf is NULL or len is 0"};
     std::string out;
     for (const dfft::Pass& q : p->passes) {
-      const char* kind = q.slab ? "slab-xy" : q.feed ? "strided-feed" : q.real ? "real-pipe"
+      const char* kind = q.slab ? "slab-xy" : q.feed ? "strided-feed" : q.async_ ? "strided-async"
+                         : q.real ? "real-pipe"
                          : q.tiled == 1 ? "tiled-contig" : q.tiled == 2 ? "tiled-strided"
                          : q.pipe ? (q.tma ? "strided-pipe" : "contig-pipe")
                          : q.is_static ? "direct" : "dynamic";

@@ -5,7 +5,7 @@
 #include <memory>
 #include <string>
 #include <vector>
-#include "tiled_pass.cuh"
+#include "async_pass.cuh"
 
 namespace dfft {
 
@@ -61,6 +61,8 @@ struct Pass {
   int tiled = 0;         // tiled_pass: 1 contiguous, 2 strided (real tensor maps)
   int tdbl = 0;          // its precision (element type of the tensor maps)
   TiledGeom tgeom{};
+  bool async_ = false;   // axis_pass_async (cp.async tiles, strides TMA cannot address)
+  AsyncGeom ageom{};
   size_t ctr_bytes = 0;  // job and per-slab counters (in the plan workspace)
   PassDesc d2{};
   SlabGeom sgeom{};
@@ -83,6 +85,8 @@ struct SlabKernel {
 const SlabKernel* find_slab_kernel(int dbl, int L, int v = 0);
 // Launch shapes of axis_pass_strided for (dbl, L), same conventions.
 const SlabKernel* find_strided_kernel(int dbl, int L, int v = 0);
+// Launch shapes of axis_pass_async (async_pass.cu); nb is unused (2 buffers).
+const SlabKernel* find_async_kernel(int dbl, int L, int v = 0);
 // real_pass kernels for half length M (fn: R2C, fn_inv: C2R), or null.
 const SlabKernel* find_real_kernel(int dbl, int M);
 // A compiled tiled_pass (tiled_pass.cu).
@@ -112,9 +116,11 @@ int choose_slab(int dbl, int L, long long O, int inverse, const std::vector<Pass
 int* device_error_word();
 
 // VARIANT_FEED: strided C2C pass with a producer warp (axis_pass_strided);
-// PassSpec::C then selects the launch shape (index into its kernel table).
+// VARIANT_ASYNC: strided C2C pass copying tiles with cp.async
+// (axis_pass_async); PassSpec::C then selects the launch shape (index into
+// the kernel's table).
 enum Variant : int { VARIANT_AUTO = 0, VARIANT_DIRECT = 1, VARIANT_PIPE = 2, VARIANT_DYNAMIC = 3,
-                     VARIANT_FEED = 4 };
+                     VARIANT_FEED = 4, VARIANT_ASYNC = 5 };
 
 // Pass construction.
 struct PassSpec {

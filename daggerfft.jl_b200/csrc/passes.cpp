@@ -375,6 +375,73 @@ static Pass make_feed_pass(const PassSpec& s) {
   return p;
 }
 
+// Strided C2C pass whose rows TMA cannot address (a row stride that is not
+// a multiple of 16 bytes): tiles copied by cp.async (axis_pass_async);
+// s.C selects the launch shape.
+static bool async_ok(const PassSpec& s, size_t esz) {
+  (void)esz;
+  return s.fast_io && !s.epi && s.I > 1 && s.I < (1LL << 31) && s.O < (1LL << 31) &&
+         find_async_kernel(s.dbl, s.L, 0) != nullptr && s.in.si == 1 && s.out.si == 1;
+}
+
+static Pass make_async_pass(const PassSpec& s) {
+  const int L = s.L;
+  const int esz = s.dbl ? 16 : 8;
+  if (!async_ok(s, esz)) throw Error{DFFT_ERROR_INVALID_VALUE, "cp.async strided variant not available"};
+  const SlabKernel* k = find_async_kernel(s.dbl, L, s.C < 0 ? 0 : s.C);
+  if (!k) throw Error{DFFT_ERROR_INVALID_VALUE, "no such cp.async launch shape"};
+  if (!s.inverse && s.scale != 1.0) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "scaled forward strided pass"};
+  const std::vector<int> rad(k->radix, k->radix + k->nst);
+  Pass p;
+  p.async_ = true;
+  p.is_static = true;
+  p.fn = s.inverse ? k->fn_inv : k->fn;
+  PassDesc& d = p.d;
+  d.L = L;
+  d.nst = k->nst;
+  int ns = 1;
+  for (int i = 0; i < d.nst; ++i) {
+    d.radix[i] = rad[i];
+    d.ns[i] = ns;
+    d.tws[i] = L / (ns * rad[i]);
+    ns *= rad[i];
+  }
+  d.P = k->P;
+  d.C = k->cs;
+  d.ld = L;
+  d.inverse = s.inverse;
+  d.cfast = 1;
+  d.Q = s.I * s.O;
+  d.I = s.I;
+  d.scale = s.scale;
+  d.in = s.in;
+  d.out = s.out;
+  for (auto& t : s.keep) p.tables.push_back(t);
+  auto stw = stage_twiddles(s.dbl, L, rad);
+  p.tables.push_back(stw);
+  d.tw = stw->p;
+  AsyncGeom& g = p.ageom;
+  g.I = s.I;
+  g.Q = s.I * s.O;
+  g.ntiles = (g.Q + k->cs - 1) / k->cs;
+  g.ntw = k->nst > 1 ? L - rad[0] : 0;
+  const size_t bstride = ((size_t)k->cs * L * esz + 127) & ~(size_t)127;
+  g.bstride = (int)(bstride / esz);
+  const size_t tw_bytes = ((size_t)g.ntw * esz + 127) & ~(size_t)127;
+  p.smem = tw_bytes + 2 * bstride;
+  p.block = dim3((unsigned)k->lb);
+  if (p.smem > max_smem_per_block()) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "strided tiles do not fit"};
+  cuda_check(ensure_smem_attr(p.fn, p.smem), "cudaFuncSetAttribute(async)");
+  int occ = 0;
+  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p.fn, (int)p.block.x, p.smem),
+             "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (occ < 1) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "cp.async kernel cannot be resident"};
+  long long nb = (long long)sm_count() * occ;
+  if (nb > g.ntiles) nb = g.ntiles;
+  p.grid = dim3((unsigned)(nb > 0 ? nb : 1));
+  return p;
+}
+
 // R2C first pass / C2R last pass over whole contiguous pencils (I = 1):
 // real_pass when a kernel exists for the half length and the pencils split
 // into whole tiles.
@@ -551,6 +618,7 @@ static Pass make_tiled_pass(const PassSpec& s) {
 
 Pass make_pass(const PassSpec& s) {
   if (s.variant == VARIANT_FEED) return make_feed_pass(s);
+  if (s.variant == VARIANT_ASYNC) return make_async_pass(s);
   if (s.variant == VARIANT_AUTO && tiled_kind(s)) {
     try {
       return make_tiled_pass(s);
@@ -587,6 +655,21 @@ Pass make_pass(const PassSpec& s) {
         if (!k->dflt || k->cs > s.I) continue;
         PassSpec t = s;
         t.variant = VARIANT_FEED;
+        t.C = v;
+        try {
+          return make_pass(t);
+        } catch (const Error&) {
+        }
+        break;
+      }
+    }
+    // the same passes with rows TMA cannot address: cp.async tiles
+    if (!feed_ok(s, esz) && (s.I * (long long)esz) % 16 != 0 && async_ok(s, esz) &&
+        (double)s.I * (double)s.O * (double)L * esz >= (double)(16 << 20)) {
+      for (int v = 0; const SlabKernel* k = find_async_kernel(s.dbl, L, v); ++v) {
+        if (!k->dflt || k->cs > s.I) continue;
+        PassSpec t = s;
+        t.variant = VARIANT_ASYNC;
         t.C = v;
         try {
           return make_pass(t);
@@ -891,6 +974,14 @@ cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream,
     if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
       return cudaErrorMisalignedAddress;
     RealGeom g = p.rgeom;
+    void* args[] = {&d, &g};
+    return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
+  }
+  if (p.async_) {
+    // the cp.async kernels move 8-byte (ComplexF32) elements
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 7)
+      return cudaErrorMisalignedAddress;
+    AsyncGeom g = p.ageom;
     void* args[] = {&d, &g};
     return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
   }

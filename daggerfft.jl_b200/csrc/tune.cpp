@@ -104,6 +104,17 @@ Pass tune_pass(const PassSpec& s) {
     } catch (const Error&) {
     }
   }
+  // cp.async strided kernels (rows TMA cannot address): one per launch shape
+  for (int i = 0; find_async_kernel(s.dbl, s.L, i); ++i) {
+    PassSpec t = s;
+    t.variant = VARIANT_ASYNC;
+    t.C = i;
+    try {
+      make_pass(t);
+      cands.push_back({VARIANT_ASYNC, i});
+    } catch (const Error&) {
+    }
+  }
   if (cands.empty()) return make_pass(s);
   const size_t ib = side_bytes(s, s.in, false), ob = side_bytes(s, s.out, true);
   void *in = nullptr, *out = nullptr;
@@ -140,7 +151,8 @@ Pass tune_pass(const PassSpec& s) {
     } catch (const Error&) {
       continue;
     }
-    if (vc.first != VARIANT_FEED && (int)p.d.C != vc.second) continue;  // clamped to another candidate
+    if (vc.first != VARIANT_FEED && vc.first != VARIANT_ASYNC && (int)p.d.C != vc.second)
+      continue;  // clamped to another candidate
     bool ok = true;
     for (int i = 0; i < 2 && ok; ++i) ok = launch_pass(p, in, out, st) == cudaSuccess;
     if (!ok) { cudaGetLastError(); continue; }
