@@ -186,6 +186,19 @@ def run_profile(args):
     shape = tuple(int(x) for x in args.shape.split(","))
     torch.cuda.set_device(0)
     g = torch.Generator(device="cuda").manual_seed(0)
+    if args.real:
+        # Float32 rfft over the --profile dims (the R2C pass first)
+        x = torch.randn(tuple(reversed(shape)), dtype=torch.float32, device="cuda", generator=g)
+        X = x.permute(*reversed(range(len(shape))))
+        dims = tuple(int(c) for c in args.profile)
+        flags = 0 if args.no_tune else dfft.FLAG_TUNE
+        p = dfft.gpu_plan_transform(dfft.RFFT(), X, dims, flags=flags)
+        Y = dfft.empty_like_layout(p.out_shape, torch.complex64, X)
+        for _ in range(2):
+            p.execute(X, Y)
+        torch.cuda.synchronize()
+        print(f"profile: rfft dims {dims} of {shape}, {p.launches} launch(es) per call, 2 calls")
+        return
     a = torch.randn(tuple(reversed(shape)), dtype=torch.complex64, device="cuda", generator=g)
     A = a.permute(*reversed(range(len(shape))))
     B = dfft.empty_like_layout(A.shape, A.dtype, A)
@@ -223,6 +236,8 @@ def main():
     ap.add_argument("--no-fuse", action="store_true",
                     help="one pass per axis (no fused dims-(1,2) slab pass)")
     ap.add_argument("--shape", default="512,512,512", help="profiling mode: ComplexF32 array shape")
+    ap.add_argument("--real", action="store_true",
+                    help="profiling mode: a Float32 rfft instead of a ComplexF32 fft")
     ap.add_argument("--slab-variant", type=int, default=-1,
                     help="profiling mode: the fused slab kernel's variant (index into its table)")
     args = ap.parse_args()

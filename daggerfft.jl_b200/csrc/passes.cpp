@@ -479,8 +479,15 @@ static Pass make_real_pass(const PassSpec& s) {
     d.tws[i] = M / (ns * rad[i]);
     ns *= rad[i];
   }
+  // work-buffer column stride: the P lanes of a pencil touch P consecutive
+  // 8-byte slots of a bank row, so pencils P slots apart (mod 16) fill the
+  // row evenly (ComplexF64: P lanes of 16 bytes fill whole rows anyway)
   int ld = swz_host(M - 1, esz) + 1;
-  if ((ld & 1) == 0) ld += 1;
+  if (esz == 8) {
+    while (ld % 16 != k->P % 16) ++ld;
+  } else if ((ld & 1) == 0) {
+    ld += 1;
+  }
   d.P = k->P;
   d.C = k->cs;
   d.ld = ld;
@@ -503,7 +510,10 @@ static Pass make_real_pass(const PassSpec& s) {
   g.ntiles = s.O / k->cs;
   g.ntw = k->nst > 1 ? M - rad[0] : 0;
   g.ld = ld;
-  const size_t bstride = ((size_t)k->cs * (M + 1) * esz + 127) & ~(size_t)127;
+  // a buffer holds the C pencils of M elements PS = M + 64 bytes apart
+  // (bank spread), or C*(M+1) dense elements
+  const size_t ps = (size_t)M + 64 / esz;
+  const size_t bstride = ((size_t)k->cs * ps * esz + 127) & ~(size_t)127;
   g.bstride = (int)(bstride / esz);
   g.err = device_error_word();
   const size_t tw_bytes = ((size_t)(g.ntw + M + 1) * esz + 127) & ~(size_t)127;

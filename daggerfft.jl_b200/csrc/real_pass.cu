@@ -29,7 +29,7 @@ DFFT_REAL_INST(double, 128, 3, 48, 6, 16, 6, 8)
 DFFT_REAL_INST(double, 96, 4, 64, 8, 8, 8, 8)
 DFFT_REAL_INST(double, 96, 4, 96, 8, 8, 12, 8)
 DFFT_REAL_INST(double, 96, 4, 128, 8, 8, 16, 8)
-DFFT_REAL_INST(double, 128, 3, 192, 12, 8, 12, 16)
+DFFT_REAL_INST(double, 128, 2, 192, 12, 8, 12, 16)
 DFFT_REAL_INST(double, 96, 4, 256, 16, 4, 16, 16)
 
 static const SlabKernel kRealKernels[] = {
@@ -46,7 +46,7 @@ static const SlabKernel kRealKernels[] = {
     {1, 64, 8, 2, {8, 8}, 96, 8, 2, 1, K(double, 96, 4, 64, 8, 8, 8, 8)},
     {1, 96, 8, 2, {12, 8}, 96, 8, 2, 1, K(double, 96, 4, 96, 8, 8, 12, 8)},
     {1, 128, 8, 2, {16, 8}, 96, 8, 2, 1, K(double, 96, 4, 128, 8, 8, 16, 8)},
-    {1, 192, 12, 2, {12, 16}, 128, 8, 2, 1, K(double, 128, 3, 192, 12, 8, 12, 16)},
+    {1, 192, 12, 2, {12, 16}, 128, 8, 2, 1, K(double, 128, 2, 192, 12, 8, 12, 16)},
     {1, 256, 16, 2, {16, 16}, 96, 4, 2, 1, K(double, 96, 4, 256, 16, 4, 16, 16)},
 };
 

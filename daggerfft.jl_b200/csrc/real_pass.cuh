@@ -13,12 +13,20 @@
 //
 // Persistent CTAs of C*P stage threads plus one producer warp.  A tile is C
 // consecutive pencils: its input and its output are each one contiguous run
-// (C*M or C*(M+1) complex elements), moved by one 1-D bulk copy into / out
-// of an NB-deep ring of tile buffers; the producer issues both copies (the
-// store when the stage threads hand the buffer back, before refilling it).  R2C: the stages read the dense tile
-// and run in a padded work buffer; the post-pass writes the M+1 outputs of
-// each pencil back into the (consumed) tile buffer.  C2R: the pre-pass reads
-// the tile and writes the work buffer; the stages end in the tile buffer.
+// in global memory (C*M or C*(M+1) complex elements), moved into / out of an
+// NB-deep ring of tile buffers by 1-D bulk copies that the producer issues
+// (the store when the stage threads hand the buffer back, before refilling
+// it).  The side of M elements per pencil sits in the buffer with the
+// pencils PS = M + 64 bytes apart (one bulk copy per pencil; M complex
+// elements are a 16-byte multiple), so the pencils a warp reads or writes
+// at once alternate between the two halves of the banks instead of all
+// mapping onto the same ones; the side of M+1 elements stays dense (one
+// bulk copy) and the pack / unpack step walks it in the flattened
+// [pencil][k] order, 32 consecutive elements per warp.  R2C: the stages read
+// the padded tile and run in a padded work buffer; the post-pass writes the
+// M+1 outputs of each pencil back into the (consumed) tile buffer.  C2R: the
+// pre-pass reads the dense tile and writes the work buffer; the stages end
+// in the padded tile.
 // The stage twiddles and the M+1 entries of w^k sit in shared memory.
 // Waits are bounded as in the other pipelined passes.
 #pragma once
@@ -44,6 +52,7 @@ __global__ void __launch_bounds__(LB, MINB) real_pass(const PassDesc d, const Re
   static_assert(NB >= 2 && NB <= 4, "tile buffers");
   constexpr int IN_E = DIR == 1 ? M : M + 1;   // complex elements per input pencil
   constexpr int OUT_E = DIR == 1 ? M + 1 : M;  // and per output pencil
+  constexpr int PS = M + 64 / (int)sizeof(V);  // pencil stride of the M-element side in a buffer
   extern __shared__ __align__(128) unsigned char smem_real[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_real);
   uint64_t* empty = reinterpret_cast<uint64_t*>(smem_real + 32);
@@ -94,7 +103,12 @@ __global__ void __launch_bounds__(LB, MINB) real_pass(const PassDesc d, const Re
       auto drain = [&](int b) -> bool {
         if (pend[b] < 0) return true;
         if (!mbar_wait_bounded(&empty[b], (uint32_t)((fills[b] - 1) & 1))) return false;
-        bulk_store_1d(dst + pend[b] * C * OUT_E, bufs + b * bst, out_bytes);
+        if constexpr (DIR == 1) {
+          bulk_store_1d(dst + pend[b] * C * OUT_E, bufs + b * bst, out_bytes);
+        } else {
+          for (int cc = 0; cc < C; ++cc)
+            bulk_store_1d(dst + (pend[b] * C + cc) * M, bufs + b * bst + cc * PS, (uint32_t)(M * sizeof(V)));
+        }
         bulk_commit();
         bulk_wait_read_all();
         pend[b] = -1;
@@ -115,7 +129,12 @@ __global__ void __launch_bounds__(LB, MINB) real_pass(const PassDesc d, const Re
           break;
         }
         mbar_expect_tx(&full[b], in_bytes);
-        bulk_load_1d(bufs + b * bst, src + tile * C * IN_E, in_bytes, &full[b]);
+        if constexpr (DIR == 1) {
+          for (int cc = 0; cc < C; ++cc)
+            bulk_load_1d(bufs + b * bst + cc * PS, src + (tile * C + cc) * M, (uint32_t)(M * sizeof(V)), &full[b]);
+        } else {
+          bulk_load_1d(bufs + b * bst, src + tile * C * IN_E, in_bytes, &full[b]);
+        }
         pend[b] = tile;
         tile += gridDim.x;
       }
@@ -140,34 +159,39 @@ __global__ void __launch_bounds__(LB, MINB) real_pass(const PassDesc d, const Re
       if (tile < 0) break;
       V* buf = bufs + b * bst;
       if constexpr (DIR == 1) {
-        const StrideCol<V> dense{buf + (size_t)c * M, 1};
+        const StrideCol<V> padded{buf + (size_t)c * PS, 1};
         static_stages<T, M, P, true, 1, NC, 1, 1, 1, 0, StrideCol<V>, PadCol<V>, PadCol<V>, StageTw<V>, Rs...>(
-            d, t, dense, pad, pad, tw, 0, 0, true);
-        // post-pass: X_k, k = 0..M, into the consumed tile buffer
-        V* o = buf + (size_t)c * (M + 1);
-        for (int k = t; k <= M; k += P) {
-          const V zk = pad.ld(k == M ? 0 : k, 0);
-          const V zm = cconj(pad.ld(k == 0 ? 0 : M - k, 0));
-          const V e = cscale(cadd(zk, zm), (T)0.5);
+            d, t, padded, pad, pad, tw, 0, 0, true);
+        // post-pass: X_k of pencil cc, k = 0..M, into the consumed tile
+        // buffer, dense: element e = cc*(M+1) + k
+        for (int e = tid; e < C * (M + 1); e += NC) {
+          const int cc = e / (M + 1), k = e - cc * (M + 1);
+          const PadCol<V> z{work + (size_t)cc * g.ld};
+          const V zk = z.ld(k == M ? 0 : k, 0);
+          const V zm = cconj(z.ld(k == 0 ? 0 : M - k, 0));
+          const V ev = cscale(cadd(zk, zm), (T)0.5);
           const V od = cscale(cmul_mi(csub(zk, zm)), (T)0.5);
-          o[k] = cscale(cadd(e, cmul(sw[k], od)), (T)d.scale);
+          buf[e] = cscale(cadd(ev, cmul(sw[k], od)), (T)d.scale);
         }
       } else {
-        // pre-pass: Z'_k, k = 0..M-1, into the work buffer
-        const V* x = buf + (size_t)c * (M + 1);
-        for (int k = t; k < M; k += P) {
+        // pre-pass: Z'_k of pencil cc, k = 0..M-1, from the dense tile
+        // (element cc*(M+1) + k) into the work buffer
+        for (int e = tid; e < C * M; e += NC) {
+          const int cc = e / M, k = e - cc * M;
+          const V* x = buf + (size_t)cc * (M + 1);
           V A = x[k];
           V B = cconj(x[M - k]);
           if (k == 0) {
             A.y = (T)0;
             B.y = (T)0;
           }
-          pad.st(k, 0, cadd(cadd(A, B), cmul_pi(cmul(cconj(sw[k]), csub(A, B)))));
+          const PadCol<V> z{work + (size_t)cc * g.ld};
+          z.st(k, 0, cadd(cadd(A, B), cmul_pi(cmul(cconj(sw[k]), csub(A, B)))));
         }
         stage_sync<NC>();
-        const StrideCol<V> dense{buf + (size_t)c * M, 1};
+        const StrideCol<V> padded{buf + (size_t)c * PS, 1};
         static_stages<T, M, P, true, 1, NC, 2, 1, 1, 0, PadCol<V>, PadCol<V>, StrideCol<V>, StageTw<V>, Rs...>(
-            d, t, pad, pad, dense, tw, 0, 0, true);
+            d, t, pad, pad, padded, tw, 0, 0, true);
       }
       fence_proxy_async_smem();  // the producer's bulk store reads the tile next
       stage_sync<NC>();
