@@ -450,7 +450,11 @@ def main():
                          "dram_floor_gbs": round(dram_floor_gbs, 1),
                          "dram_floor_frac": round(dram_floor_gbs / peak, 4),
                          "per_launch_ms": {",".join(map(str, k)): round(v[0], 4) for k, v in per_launch.items()},
-                         "step_frac_of_peak": round(value / world / peak, 4)},
+                         "step_frac_of_peak": round(value / world / peak, 4),
+                         # B200 HBM3e nominal 8 TB/s, for context beside the measured peak
+                         "nominal_gbs": 8000.0,
+                         "frac_of_nominal": round(achieved / 8000.0, 4),
+                         "step_frac_of_nominal": round(value / world / 8000.0, 4)},
             "e2e": {"value": round(e2e, 2), "unit": "GB/s", "ms_per_step": round(e2e_ms, 3),
                     "h2d_bytes_per_step": FIELD_BYTES, "d2h_bytes_per_step": FIELD_BYTES,
                     "overlap": "double-buffered: upload i+1 / transforms i / download i-1 on three streams",
