@@ -31,6 +31,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <type_traits>
 #include "codelets.cuh"
 
 namespace dfft {
@@ -337,6 +338,13 @@ template <typename V> struct StageTw {
     return p[off + jm * (R - 1) + r - 1];
   }
 };
+// The same table with the last stage's entries pre-multiplied by the
+// inverse's 1/L (exact for power-of-two L): the last stage of an inverse
+// then scales only its r = 0 inputs, and the DFT carries the scale to every
+// output (linearity), instead of scaling every output.
+template <typename V> struct StageTwScaledLast : StageTw<V> {};
+template <class TW> struct scaled_last_tw { static constexpr bool value = false; };
+template <typename V> struct scaled_last_tw<StageTwScaledLast<V>> { static constexpr bool value = true; };
 // Twiddles computed in the kernel (no table in memory): exp(-2 pi i jm r ts / L)
 // with the CUDA math library's sincospi in double precision.
 template <typename V> struct ComputedTw {
@@ -385,7 +393,10 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
   // direction: at run time (DIR 0), or compiled in (1 forward: no
   // conjugation, unit scale; 2 inverse)
   const bool inv = DIR == 0 ? d.inverse != 0 : DIR == 2;
-  const T scale = DIR == 1 ? (T)1 : (T)d.scale;
+  // scale folded into the last stage's twiddles (inverse kernels whose
+  // table says so): only the r = 0 inputs are scaled here
+  const bool fold = scaled_last_tw<TW>::value && DIR == 2 && last && !first;
+  const T scale = DIR == 1 || fold ? (T)1 : (T)d.scale;
   const bool to_global = SMEM_IO != 1 && last && !d.epi;
   const bool from_global = SMEM_IO == 0 && first;
   V v[BMAX][R];
@@ -420,6 +431,7 @@ __device__ __forceinline__ void stage_body(const PassDesc& d, int L, int P, int 
       if (!first) {
 #pragma unroll
         for (int r = 1; r < R; ++r) v[b][r] = cmul(v[b][r], tw.w(toff, jm, r, R, ts));
+        if (fold) v[b][0] = cscale(v[b][0], (T)d.scale);
       }
       Dft<R>::run(v[b]);
       const int o0 = (j - jm) * R + jm;

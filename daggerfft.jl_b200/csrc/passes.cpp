@@ -246,13 +246,16 @@ static size_t max_smem_per_block() {
 }
 
 // Stage-major twiddle table for a radix sequence (StageTw layout): entry
-// Ns - R_0 + jm*(R-1) + r-1 of stage s >= 1 is exp(-2 pi i jm r / (Ns R)).
-static std::shared_ptr<DevTable> stage_twiddles(int dbl, int L, const std::vector<int>& rad) {
+// Ns - R_0 + jm*(R-1) + r-1 of stage s >= 1 is exp(-2 pi i jm r / (Ns R)),
+// times last_scale in the last stage (StageTwScaledLast: the inverse's 1/L
+// folded into the table).
+static std::shared_ptr<DevTable> stage_twiddles(int dbl, int L, const std::vector<int>& rad,
+                                                double last_scale = 1.0) {
   static std::mutex mu;
-  static std::map<std::tuple<int, int, std::vector<int>>, std::weak_ptr<DevTable>> cache;
+  static std::map<std::tuple<int, int, std::vector<int>, double>, std::weak_ptr<DevTable>> cache;
   int dev = 0;
   cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-  auto key = std::make_tuple(dev * 2 + dbl, L, rad);
+  auto key = std::make_tuple(dev * 2 + dbl, L, rad, last_scale);
   std::lock_guard<std::mutex> lk(mu);
   auto it = cache.find(key);
   if (it != cache.end())
@@ -270,7 +273,8 @@ static std::shared_ptr<DevTable> stage_twiddles(int dbl, int L, const std::vecto
         const long long D = (long long)Ns * R;
         const long long m = ((long long)jm * r) % D;
         const long double ang = two_pi * (long double)m / (long double)D;
-        const long double c = cosl(ang), sn = -sinl(ang);
+        const long double f = st + 1 == rad.size() ? (long double)last_scale : 1.0L;
+        const long double c = f * cosl(ang), sn = -f * sinl(ang);
         const size_t e = (size_t)(Ns - R0 + jm * (R - 1) + r - 1);
         if (dbl) { double v[2] = {(double)c, (double)sn}; std::memcpy(&host[esz * e], v, esz); }
         else { float v[2] = {(float)c, (float)sn}; std::memcpy(&host[esz * e], v, esz); }
@@ -906,7 +910,8 @@ Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v) {
   };
   fill(p.d, 1);
   fill(p.d2, L);
-  auto stw = stage_twiddles(dbl, L, rad);
+  // the inverse kernels fold 1/L into the last stage's twiddles
+  auto stw = stage_twiddles(dbl, L, rad, inverse ? 1.0 / (double)L : 1.0);
   p.tables.push_back(stw);
   p.d.tw = stw->p;
   auto twl = twiddle_table(dbl, L, 1, 0, L, false);

@@ -270,7 +270,10 @@ __global__ void __launch_bounds__(LB, MINB)
   } else {
     // ---------------- stage threads ----------------
     // both phases have the same length and radices: one stage-twiddle table
-    const StageTw<V> tw{stw};
+    // (for the inverse, with 1/L folded into the last stage's entries; both
+    // phases scale by 1/L)
+    typedef typename std::conditional<DIR == 2, StageTwScaledLast<V>, StageTw<V>>::type TWT;
+    const TWT tw{stw};
     constexpr int R0 = first_radix<Rs...>::value;
     for (int it = 0;; ++it) {
       const int b = it % NB;
@@ -286,14 +289,14 @@ __global__ void __launch_bounds__(LB, MINB)
         const XSwzCol<V, L, R0> sw{buf + (size_t)c * L, c};
         const long long ob = ((long long)J.slab * L + (long long)J.tile * CS + c) * L;
         static_stages<T, L, P, true, 2, NC, DIR, 1, 1, 0, StrideCol<V>, XSwzCol<V, L, R0>, XSwzCol<V, L, R0>,
-                      StageTw<V>, Rs...>(dx, t, dense, sw, sw, tw, 0, ob, true);
+                      TWT, Rs...>(dx, t, dense, sw, sw, tw, 0, ob, true);
         fence_proxy_async_global();  // these stores are read by bulk-tensor loads
       } else {
         const int c = tid % CS, t = tid / CS;
         const StrideColC<V, CS> dense{buf + c};
         const YSwzCol<V, CS, R0> sw{buf + c};
         static_stages<T, L, P, true, 1, NC, DIR, 1, 1, 0, StrideColC<V, CS>, YSwzCol<V, CS, R0>, StrideColC<V, CS>,
-                      StageTw<V>, Rs...>(dy, t, dense, sw, dense, tw, 0, 0, true);
+                      TWT, Rs...>(dy, t, dense, sw, dense, tw, 0, 0, true);
       }
       fence_proxy_async_smem();  // the buffer is next read (store) or written (load) by TMA
       stage_sync<NC>();
