@@ -8,10 +8,10 @@
 // Persistent CTAs of CS*P threads, all of which run the stages.  A tile is
 // CS consecutive columns of the flattened column index q = qi + I*qo (so no
 // tile is left partly empty at the end of each run of I columns) x L rows;
-// every thread copies its share of the NEXT tile into the other of two
-// shared buffers with 8- or 16-byte cp.async (zero-filled past the last
-// column) before it transforms the current one, so the copy of tile i+1
-// overlaps the stages of tile i.  The first stage reads the dense [row][column]
+// every thread copies its share of tile i+NB-1 into a ring of NB shared
+// buffers with 8- or 16-byte cp.async (zero-filled past the last column)
+// before it transforms tile i, so the copies of the next NB-1 tiles overlap
+// the stages of the current one.  The first stage reads the dense [row][column]
 // tile, the middle stages run in the row-swizzled layout with the stage
 // twiddles in shared memory, and the last stage stores straight to global
 // memory, CS consecutive elements per row (coalesced, 8-byte aligned).
@@ -27,7 +27,7 @@ struct AsyncGeom {
   long long Q;       // columns: I * O
   long long I;       // columns along the contiguous axes
   int ntw;           // stage-twiddle entries
-  int bstride;       // elements between the two tile buffers (128-byte multiple)
+  int bstride;       // elements between the tile buffers (128-byte multiple)
 };
 
 // cp.async of one element (8 or 16 bytes); src_bytes 0 fills zeros
@@ -45,10 +45,11 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <typename T, int LB, int MINB, int DIR, int L, int P, int CS, int... Rs>
+template <typename T, int LB, int MINB, int NB, int DIR, int L, int P, int CS, int... Rs>
 __global__ void __launch_bounds__(LB, MINB) axis_pass_async(const PassDesc d, const AsyncGeom g) {
   typedef typename cvec<T>::type V;
   static_assert(CS * P == LB, "every thread runs the stages");
+  static_assert(NB >= 2 && NB <= 4, "tile buffers");
   static_assert((CS * L) % LB == 0, "whole copy rounds");
   constexpr int R0 = first_radix<Rs...>::value;
   constexpr bool kPow2 = (L & (L - 1)) == 0 && (((Rs & (Rs - 1)) == 0) && ...);
@@ -76,15 +77,20 @@ __global__ void __launch_bounds__(LB, MINB) axis_pass_async(const PassDesc d, co
     for (int i = 0; i < CS * L / LB; ++i) cp_async_elem<sizeof(V)>(buf + tid + i * LB, s + i * rstep, ok);
   };
   const long long first = blockIdx.x, step = gridDim.x;
-  if (first < g.ntiles) issue(first, bufs);
-  cp_async_commit();
+  // prologue: tiles 0 .. NB-2 of this CTA, one commit group each
+#pragma unroll
+  for (int i = 0; i < NB - 1; ++i) {
+    if (first + i * step < g.ntiles) issue(first + i * step, bufs + (size_t)i * g.bstride);
+    cp_async_commit();
+  }
   int it = 0;
   for (long long tile = first; tile < g.ntiles; tile += step, ++it) {
-    V* buf = bufs + (size_t)(it & 1) * g.bstride;
-    if (tile + step < g.ntiles) issue(tile + step, bufs + (size_t)((it + 1) & 1) * g.bstride);
+    V* buf = bufs + (size_t)(it % NB) * g.bstride;
+    const long long ahead = tile + (long long)(NB - 1) * step;
+    if (ahead < g.ntiles) issue(ahead, bufs + (size_t)((it + NB - 1) % NB) * g.bstride);
     cp_async_commit();
-    cp_async_wait<1>();  // this thread's copies of the current tile have landed
-    __syncthreads();     // and everyone else's (and, first time, the twiddles)
+    cp_async_wait<NB - 1>();  // this thread's copies of the current tile have landed
+    __syncthreads();          // and everyone else's (and, first time, the twiddles)
     const long long q = tile * CS + c;
     const bool cv = q < g.Q;
     const long long ob = cv ? (q % g.I) * d.out.si + (q / g.I) * d.out.so : 0;
@@ -97,7 +103,7 @@ __global__ void __launch_bounds__(LB, MINB) axis_pass_async(const PassDesc d, co
       static_stages<T, L, P, true, 3, 0, DIR, 1, 1, 0, StrideColC<V, CS>, StrideColC<V, CS>, StrideColC<V, CS>,
                     StageTw<V>, Rs...>(d, t, dense, dense, dense, tw, 0, ob, cv);
     }
-    __syncthreads();  // the buffer is refilled by the next iteration's copies
+    __syncthreads();  // the next iteration's copies refill the buffer of tile i-1
   }
   cp_async_wait<0>();
 }

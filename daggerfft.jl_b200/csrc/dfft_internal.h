@@ -85,7 +85,7 @@ struct SlabKernel {
 const SlabKernel* find_slab_kernel(int dbl, int L, int v = 0);
 // Launch shapes of axis_pass_strided for (dbl, L), same conventions.
 const SlabKernel* find_strided_kernel(int dbl, int L, int v = 0);
-// Launch shapes of axis_pass_async (async_pass.cu); nb is unused (2 buffers).
+// Launch shapes of axis_pass_async (async_pass.cu), same conventions.
 const SlabKernel* find_async_kernel(int dbl, int L, int v = 0);
 // real_pass kernels for half length M (fn: R2C, fn_inv: C2R), or null.
 const SlabKernel* find_real_kernel(int dbl, int M);

@@ -432,7 +432,7 @@ static Pass make_async_pass(const PassSpec& s) {
   const size_t bstride = ((size_t)k->cs * L * esz + 127) & ~(size_t)127;
   g.bstride = (int)(bstride / esz);
   const size_t tw_bytes = ((size_t)g.ntw * esz + 127) & ~(size_t)127;
-  p.smem = tw_bytes + 2 * bstride;
+  p.smem = tw_bytes + (size_t)k->nb * bstride;
   p.block = dim3((unsigned)k->lb);
   if (p.smem > max_smem_per_block()) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "strided tiles do not fit"};
   cuda_check(ensure_smem_attr(p.fn, p.smem), "cudaFuncSetAttribute(async)");
