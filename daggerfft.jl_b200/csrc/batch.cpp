@@ -4,7 +4,8 @@
 // A batch holds N plans (any shapes, kinds and precisions).  The first
 // execute with a given set of buffers captures every plan's passes into a
 // graph: the plans are spread over up to kBatchStreams forked capture
-// streams, so transforms of different grids become independent branches the
+// streams (fewer for large grids, see branch_count), so transforms of
+// different grids become independent branches the
 // GPU runs concurrently (the persistent pipelined kernels of one branch and
 // the one-tile kernels of another share the SMs).  Later executes with the
 // same buffers replay the instantiated graph with one cudaGraphLaunch; new
@@ -45,12 +46,35 @@ struct Batch {
   }
 };
 
+// Branches of the graph: enough concurrent transforms to fill the GPU with
+// small grids, few enough that the buffers of the transforms in flight (in +
+// out) stay resident in L2 between a transform's passes, which read what the
+// previous pass just wrote: 0.8 x L2 / the mean per-plan bytes, 2..8.  64
+// uneven ComplexF32 grids of 12 MB on average (B200, one graph launch):
+// 1.08 / 0.96 / 0.94 / 0.96 / 1.05 / 1.22 ms with 2 / 3 / 4 / 5 / 6 / 8
+// branches; this rule picks 4.
+static int branch_count(const Batch* B) {
+  const int n = (int)B->plans.size();
+  double total = 0;
+  for (const Plan* p : B->plans) total += (double)(p->in_bytes() + p->out_bytes());
+  int l2 = 0;
+  if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, B->device) != cudaSuccess) {
+    cudaGetLastError();
+    l2 = 0;
+  }
+  int k = kBatchStreams;
+  if (n > 0 && total > 0 && l2 > 0) k = (int)(0.8 * (double)l2 / (total / n));
+  if (k < 2) k = 2;
+  if (k > kBatchStreams) k = kBatchStreams;
+  return k < n ? k : n;
+}
+
 // Records the batch into a graph on the batch's own capture stream (nothing
 // runs; the graph is launched on the caller's stream afterwards).
 static void capture(Batch* B, const void* const* ins, void* const* outs, cudaGraph_t* g) {
   cudaStream_t s = B->cap;
   const int n = (int)B->plans.size();
-  const int k = n < kBatchStreams ? n : kBatchStreams;
+  const int k = branch_count(B);
   cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
   cudaError_t err = cudaSuccess;
   try {
