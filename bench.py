@@ -22,7 +22,17 @@ cpu_baseline: the oracle's restatement of the reference CPU pipeline
          block redistribution), one forward+inverse of the same 512^3 field.
 
 --impl reference times that CPU pipeline alone (rank 0), one forward+inverse
-per step, and prints its own JSON line.
+per step, and prints its own JSON line (same metric, unit and workload).
+
+errors : relative L2 of the forward result against a float64 host fftn
+         (scipy.fft on all host cores) of the same input, of the inverse
+         result against the host ifftn of the GPU's forward output, and of
+         the round trip against the input.
+configs: (one GPU) the other configured workloads, each with its time,
+         algorithmic GB/s and errors against a float64 host evaluation:
+         c1 128^3 ComplexF64 Pencil, c2 256^3 Float64/Float32 rfft+irfft,
+         c4 64 uneven ComplexF32 grids as one batch launch + the DCT-II/III
+         Float64 stack, c5 serving p50/p99 latency per Poisson arrival rate.
 
 Multi-GPU (torchrun): every rank transforms its own 512^3 field (weak
 scaling, replicas: no data-path collective); timing is the max over ranks.
@@ -44,6 +54,8 @@ FIELD_BYTES = N ** 3 * 8                     # ComplexF32
 STEP_BYTES = 2 * 3 * 2 * FIELD_BYTES         # fwd + inv, 3 passes, read + write
 PASS_BYTES = 2 * FIELD_BYTES                 # one axis pass
 CPU_CHUNK = 64
+WORKLOAD = "512^3 ComplexF32 C2C fft+ifft, decomp=Slab(), dims=(1,2,3)"
+METRIC = "512^3 C2C FFT GB/s (fwd+inv, algorithmic bytes)"
 
 
 def measured_peak():
@@ -162,12 +174,12 @@ def run_reference(args, rank, world):
     t = sum(ts) / len(ts)
     v = STEP_BYTES / t / 1e9
     line = {
-        "impl": "reference", "metric": "512^3 C2C FFT GB/s (fwd+inv, algorithmic bytes)",
+        "impl": "reference", "metric": METRIC,
         "value": round(v, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "complex64 (f32)", "data": "synthetic",
-        "config": {"workload": "512^3 ComplexF32 C2C fft+ifft, Slab(), Blocks(512,512,64)",
-                   "global_batch": 1, "seq_len": N, "parallelism": "host threads"},
+        "config": {"workload": WORKLOAD, "method": "plain", "global_batch": 1, "seq_len": N,
+                   "parallelism": "host threads", "chunks": "Blocks(512,512,64)"},
         "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": workers, "kind": "port",
                          "sample": "one full 512^3 forward+inverse per step (oracle Slab pipeline, "
                                    "pocketfft stand-in for FFTW)"},
@@ -175,6 +187,49 @@ def run_reference(args, rank, world):
         "gflops": round(5 * N ** 3 * 27 * 1e-9 / (t / 2), 2),
     }
     print(json.dumps(line), flush=True)
+
+
+def host_errors(A_host, Fd, Bd):
+    """Forward result Fd against a float64 host fftn of the input, inverse
+    result Bd against the host ifftn of Fd (scipy.fft, all host cores).
+    A_host is the pinned (z, y, x) C-order copy of the logical (x, y, z)
+    input, so the transforms run over all three axes of the same memory."""
+    import numpy as np
+    import scipy.fft
+    w = os.cpu_count() or 1
+
+    def rel(a, b):
+        num = den = 0.0
+        for k in range(0, a.shape[0], 32):
+            x = a[k:k + 32].astype(np.complex128)
+            y = b[k:k + 32]
+            num += float(np.sum(np.abs(x - y) ** 2))
+            den += float(np.sum(np.abs(y) ** 2))
+        return float(np.sqrt(num / den))
+
+    a = A_host.numpy().astype(np.complex128)
+    ref = scipy.fft.fftn(a, workers=w, overwrite_x=True)
+    del a
+    F = Fd.permute(2, 1, 0).cpu().numpy()          # (z, y, x) C order, as A_host
+    e_fwd = rel(F, ref)
+    del ref
+    inv = scipy.fft.ifftn(F.astype(np.complex128), workers=w, overwrite_x=True)
+    e_inv = rel(Bd.permute(2, 1, 0).cpu().numpy(), inv)
+    return {"fwd_rel_l2_vs_host_fp64": e_fwd, "inv_rel_l2_vs_host_fp64": e_inv,
+            "host_oracle": f"scipy.fft float64, {w} threads"}
+
+
+def run_configs():
+    import bench_configs as bc
+    out = {}
+    for name in ("c1", "c2", "c4", "c5"):
+        t0 = time.perf_counter()
+        try:
+            out[name] = getattr(bc, name)()
+        except Exception as e:  # one failing configuration does not drop the headline
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["wall_s"] = round(time.perf_counter() - t0, 1)
+    return out
 
 
 def run_profile(args):
@@ -229,6 +284,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--method", default="plain", choices=["plain", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configured workloads (c1, c2, c4, c5)")
     ap.add_argument("--no-tune", action="store_true", help="heuristic launch shapes, no autotuning")
     ap.add_argument("--profile", default="",
                     help="profiling mode: run the plan over these dims twice and exit "
@@ -317,13 +374,10 @@ def main():
         t_ms = float(tt.item())
     value = world * STEP_BYTES / (t_ms * 1e-3) / 1e9
 
-    # accuracy: round trip, and forward vs the FP64 path of this library
+    # accuracy against a float64 host evaluation of the same input
     rt = float(torch.linalg.vector_norm(Cd - Ad) / torch.linalg.vector_norm(Ad))
-    A64 = Ad.to(torch.complex128)
-    F64 = dfft.fft(A64, decomp=decomp, dims=(1, 2, 3))
-    fwd_err = float(torch.linalg.vector_norm(Bd.to(torch.complex128) - F64) / torch.linalg.vector_norm(F64))
-    del A64, F64
-    torch.cuda.empty_cache()
+    errors = host_errors(A_host, Bd, Cd) if rank == 0 else {}
+    errors["roundtrip_rel_l2"] = rt
 
     # the step's launches timed alone (roofline of the dominant one): the
     # forward plan is either the fused dims-(1,2) slab pass + the dim-3 pass,
@@ -430,16 +484,28 @@ def main():
                "sample": "one 512^3 ComplexF32 forward+inverse (oracle Slab pipeline: Blocks(512,512,64) "
                          "chunks, pocketfft per chunk with all host threads, block redistribution)"}
 
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        # the other configured workloads: the 512^3 buffers are freed first
+        # (the serving arena takes 16 GiB)
+        del Ad, Bd, Cd, pf, pi, sets
+        import gc
+        gc.collect()
+        dfft.gpu_cleanup_plans()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        configs = run_configs()
+
     if pg:
         pg.barrier()
     if rank == 0:
         line = {
-            "metric": "512^3 C2C FFT GB/s (fwd+inv, algorithmic bytes)",
+            "metric": METRIC,
             "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t_ms, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "complex64 (f32)",
             "data": "synthetic",
-            "config": {"workload": "512^3 ComplexF32 C2C fft+ifft, decomp=Slab(), dims=(1,2,3)",
+            "config": {"workload": WORKLOAD,
                        "method": args.method, "global_batch": world, "seq_len": N,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs (1 GiB) larger than L2 (126 MB); no flush needed"},
@@ -462,9 +528,11 @@ def main():
             "cpu_baseline": cpu,
             "gpu_launches": launches_per_step * args.steps,
             "gflops": round(5 * N ** 3 * 27 * 1e-9 / (t_ms * 1e-3 / 2), 1),
-            "errors": {"roundtrip_rel_l2": rt, "fwd_rel_l2_vs_fp64": fwd_err},
+            "errors": errors,
             "clocks": clk,
         }
+        if configs is not None:
+            line["configs"] = configs
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()

@@ -16,8 +16,13 @@
       throughput per rate.
 
 Usage: python daggerfft.jl_b200/bench_configs.py [c1 c2 c4 ...]
+(bench.py runs the same functions and puts their dicts in its JSON line).
 Times are CUDA-event averages after warm-up; bytes are algorithmic (one
-read + one write of the field per axis pass).
+read + one write of the field per axis pass).  Every error is a relative L2
+against a float64 host evaluation (scipy.fft / pocketfft on all host
+cores) of the same input: the forward result against fftn / rfftn / dctn,
+the inverse result against the host inverse of the GPU's own forward
+output, and the round trip against the input.
 """
 import json
 import os
@@ -57,7 +62,29 @@ def rel(a, b):
                  torch.linalg.vector_norm(b.to(torch.complex128)))
 
 
-def c1():
+WORKERS = os.cpu_count() or 1
+
+
+def host(t):
+    """Host float64 / complex128 copy of a device tensor, logical indexing."""
+    x = t.detach().cpu().numpy()
+    return x.astype(np.complex128 if np.iscomplexobj(x) else np.float64)
+
+
+def hrel(a, b):
+    """Relative L2 of host arrays (float64 accumulation)."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.sqrt(np.sum(np.abs(a - b) ** 2) / np.sum(np.abs(b) ** 2)))
+
+
+def sfft():
+    import scipy.fft
+    return scipy.fft
+
+
+def c1(cpu=True):
+    """128^3 ComplexF64 fft + ifft, Pencil, U[0,1) real and imaginary parts."""
     n = 128
     g = torch.Generator(device="cuda").manual_seed(1)
     A = fcol(torch.complex(torch.rand((n, n, n), device="cuda", dtype=torch.float64, generator=g),
@@ -68,26 +95,38 @@ def c1():
     pi = dfft.gpu_plan_transform(dfft.IFFT(), B, (1, 2, 3), decomp=dfft.Pencil(), flags=dfft.FLAG_TUNE)
     ms = timed(lambda: (pf.execute(A, B), pi.execute(B, C)))
     step_bytes = 2 * 3 * 2 * n ** 3 * 16
-    # the CPU pipeline of the reference (oracle port), one fwd+inv
-    sys.path.insert(0, os.path.join(HERE, "..", "oracle"))
-    import dfft_oracle as oracle
-    oracle.WORKERS = os.cpu_count() or 1
-    a = A.cpu().numpy()
-    DA, DB, DC = oracle.pencil_layouts((n, n, n), 32, 1)
-    oracle.distribute(a, DA)
-    ws = [oracle.create_workspace(DA, DB, 0)], [oracle.create_workspace(DB, DC, 0)]
-    t0 = time.perf_counter()
-    oracle.fft_pencil(DC, DA, DB, ws[0], ws[1], (oracle.FFT_(),) * 3, (1, 2, 3), precision="native")
-    t_cpu_f = time.perf_counter() - t0
-    err = oracle.rel_l2(oracle.collect(DC), np.fft.fftn(a))
-    print(json.dumps({"config": "c1 128^3 ComplexF64 fft+ifft Pencil", "gpu_ms_per_fwd_inv": round(ms, 4),
-                      "gpu_GBps": round(step_bytes / ms / 1e6, 1),
-                      "cpu_ms_fwd": round(t_cpu_f * 1e3, 2), "cpu_threads": oracle.WORKERS,
-                      "roundtrip_rel_l2": rel(C, A), "cpu_fwd_rel_l2_vs_fftn": err}), flush=True)
+    pf.execute(A, B)
+    pi.execute(B, C)
+    torch.cuda.synchronize()
+    a, Bh, Ch = host(A), host(B), host(C)
+    fx = sfft()
+    out = {"config": "c1 128^3 ComplexF64 fft+ifft Pencil, U[0,1)", "ms_per_fwd_inv": round(ms, 4),
+           "GBps": round(step_bytes / ms / 1e6, 1),
+           "fwd_rel_l2_vs_host_fp64": hrel(Bh, fx.fftn(a, workers=WORKERS)),
+           "inv_rel_l2_vs_host_fp64": hrel(Ch, fx.ifftn(Bh, workers=WORKERS)),
+           "roundtrip_rel_l2": hrel(Ch, a)}
+    if cpu:
+        # the reference's CPU pipeline (the oracle's Pencil restatement,
+        # Blocks(128,32,32), pocketfft per chunk on all host threads), one forward
+        sys.path.insert(0, os.path.join(HERE, "..", "oracle"))
+        import dfft_oracle as oracle
+        oracle.WORKERS = WORKERS
+        DA, DB, DC = oracle.pencil_layouts((n, n, n), 32, 1)
+        oracle.distribute(a, DA)
+        ws = [oracle.create_workspace(DA, DB, 0)], [oracle.create_workspace(DB, DC, 0)]
+        t0 = time.perf_counter()
+        oracle.fft_pencil(DC, DA, DB, ws[0], ws[1], (oracle.FFT_(),) * 3, (1, 2, 3), precision="native")
+        t_cpu_f = time.perf_counter() - t0
+        out["cpu_baseline"] = {"ms_fwd": round(t_cpu_f * 1e3, 2), "threads": WORKERS, "kind": "port",
+                               "sample": "one 128^3 forward (oracle Pencil pipeline, pocketfft stand-in for FFTW)"}
+    return out
 
 
 def c2():
+    """256^3 Float64 and Float32 rfft + irfft, Pencil, U[0,1)."""
     n = 256
+    res = []
+    fx = sfft()
     for dt in (torch.float64, torch.float32):
         g = torch.Generator(device="cuda").manual_seed(2)
         A = fcol(torch.rand((n, n, n), device="cuda", dtype=dt, generator=g))
@@ -102,15 +141,25 @@ def c2():
         h = n // 2 + 1
         fwd = n ** 3 * sr + h * n * n * sc + 2 * 2 * h * n * n * sc
         step = 2 * fwd
-        # forward vs the FP64 path of this library on the same input
-        F64 = dfft.rfft(A.to(torch.float64), dims=(1, 2, 3))
-        print(json.dumps({"config": f"c2 256^3 {'Float64' if dt == torch.float64 else 'Float32'} rfft+irfft Pencil",
-                          "ms_per_fwd_inv": round(ms, 4), "GBps": round(step / ms / 1e6, 1),
-                          "fwd_rel_l2_vs_fp64": rel(F.to(torch.complex128), F64),
-                          "roundtrip_rel_l2": rel(X, A)}), flush=True)
+        pf.execute(A, F)
+        pi.execute(F, X)
+        torch.cuda.synchronize()
+        a, Fh, Xh = host(A), host(F), host(X)
+        # rfft halves the first (logical) axis: the real transform runs over
+        # the last axis listed
+        ref = fx.rfftn(a, axes=(2, 1, 0), workers=WORKERS)
+        inv = fx.irfftn(Fh, s=(n, n, n), axes=(2, 1, 0), workers=WORKERS)
+        res.append({"precision": "Float64" if dt == torch.float64 else "Float32",
+                    "ms_per_fwd_inv": round(ms, 4), "GBps": round(step / ms / 1e6, 1),
+                    "fwd_rel_l2_vs_host_fp64": hrel(Fh, ref),
+                    "inv_rel_l2_vs_host_fp64": hrel(Xh, inv),
+                    "roundtrip_rel_l2": hrel(Xh, a)})
+    return {"config": "c2 256^3 rfft+irfft Pencil, U[0,1)", "results": res}
 
 
 def c4():
+    """64 uneven ComplexF32 grids as one batch launch, and the 2-D
+    DCT-II / DCT-III Float64 256 x 256 x 32 stack."""
     edges = [48, 64, 80, 96, 120, 128, 160, 192]
     rng = np.random.default_rng(4)
     shapes = [tuple(int(e) for e in rng.choice(edges, 3)) for _ in range(64)]
@@ -123,6 +172,10 @@ def c4():
     batch = dfft.Batch(plans)
     ms_graph = timed(lambda: batch.execute(ins, outs))
     ms_seq = timed(lambda: [p.execute(x, o) for p, x, o in zip(plans, ins, outs)])
+    batch.execute(ins, outs)
+    torch.cuda.synchronize()
+    fx = sfft()
+    err = max(hrel(host(o), fx.fftn(host(x), workers=WORKERS)) for x, o in zip(ins, outs))
     elems = sum(a * b * c for a, b, c in shapes)
     byts = 3 * 2 * elems * 8
     # DCT-II / DCT-III Float64 256x256 x 32 (dims 1,2)
@@ -132,16 +185,23 @@ def c4():
     E = dfft.empty_like_layout(D.shape, D.dtype, D)
     R = dfft.empty_like_layout(D.shape, D.dtype, D)
     ms_dct = timed(lambda: (p2.execute(D, E), p3.execute(E, R)))
+    p2.execute(D, E)
+    p3.execute(E, R)
+    torch.cuda.synchronize()
     dbytes = 2 * 2 * 2 * 256 * 256 * 32 * 8
-    err = rel(R / (4 * 256 * 256), D)
-    print(json.dumps({"config": "c4 64 uneven C2C ComplexF32 grids, one graph launch",
-                      "grids": len(shapes), "elements": elems, "kernel_launches_in_graph": batch.launches,
-                      "ms_graph": round(ms_graph, 4), "ms_sequential_launches": round(ms_seq, 4),
-                      "GBps_graph": round(byts / ms_graph / 1e6, 1),
-                      "GBps_sequential": round(byts / ms_seq / 1e6, 1),
-                      "dct2_dct3_256x256x32_f64_ms": round(ms_dct, 4),
-                      "dct_GBps": round(dbytes / ms_dct / 1e6, 1),
-                      "dct_roundtrip_rel_l2": err}), flush=True)
+    d, Eh, Rh = host(D), host(E), host(R)
+    # scipy's unnormalised DCT-II / DCT-III are FFTW's REDFT10 / REDFT01
+    return {"config": "c4 64 uneven C2C ComplexF32 grids, one graph launch; DCT-II/III Float64 256x256x32",
+            "grids": len(shapes), "elements": elems, "kernel_launches_in_graph": batch.launches,
+            "ms_graph": round(ms_graph, 4), "ms_sequential_launches": round(ms_seq, 4),
+            "GBps_graph": round(byts / ms_graph / 1e6, 1),
+            "GBps_sequential": round(byts / ms_seq / 1e6, 1),
+            "grids_worst_fwd_rel_l2_vs_host_fp64": err,
+            "dct2_dct3_256x256x32_f64_ms": round(ms_dct, 4),
+            "dct_GBps": round(dbytes / ms_dct / 1e6, 1),
+            "dct2_rel_l2_vs_host_fp64": hrel(Eh, fx.dctn(d, type=2, axes=(0, 1), workers=WORKERS)),
+            "dct3_rel_l2_vs_host_fp64": hrel(Rh, fx.dctn(Eh, type=3, axes=(0, 1), workers=WORKERS)),
+            "dct_roundtrip_rel_l2": hrel(Rh / (4 * 256 * 256), d)}
 
 
 def c5(rates=(250, 500, 1000, 2000, 4000), seconds=2.0, budget=16 << 30, slots=8):
@@ -223,13 +283,13 @@ def c5(rates=(250, 500, 1000, 2000, 4000), seconds=2.0, budget=16 << 30, slots=8
                         "throughput_req_per_s": round(st["completed"] / st["elapsed_s"], 1),
                         "io_GBps": round(st["bytes_moved"] / st["elapsed_s"] / 1e9, 2),
                         "peak_running": st["peak_running"], "arena_peak_GB": round(st["arena_peak_bytes"] / 1e9, 2)})
-    print(json.dumps({"config": "c5 serving, Poisson arrivals, mixed fft/ifft/rfft/irfft",
-                      "slots": slots, "hbm_budget_GB": budget / 1e9, "seconds_per_rate": seconds,
-                      "rates": results}), flush=True)
     srv.close()
+    return {"config": "c5 serving, Poisson arrivals, mixed fft/ifft/rfft/irfft",
+            "slots": slots, "hbm_budget_GB": budget / 1e9, "seconds_per_rate": seconds,
+            "rates": results}
 
 
 if __name__ == "__main__":
     todo = sys.argv[1:] or ["c1", "c2", "c4"]
     for name in todo:
-        globals()[name]()
+        print(json.dumps(globals()[name]()), flush=True)

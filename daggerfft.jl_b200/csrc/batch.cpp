@@ -16,6 +16,7 @@
 #include <cstring>
 #include <mutex>
 #include <vector>
+#include "batch_rule.h"
 #include "dfft.h"
 #include "dfft_plan.h"
 
@@ -46,13 +47,8 @@ struct Batch {
   }
 };
 
-// Branches of the graph: enough concurrent transforms to fill the GPU with
-// small grids, few enough that the buffers of the transforms in flight (in +
-// out) stay resident in L2 between a transform's passes, which read what the
-// previous pass just wrote: 0.8 x L2 / the mean per-plan bytes, 2..8.  64
-// uneven ComplexF32 grids of 12 MB on average (B200, one graph launch):
-// 1.08 / 0.96 / 0.94 / 0.96 / 1.05 / 1.22 ms with 2 / 3 / 4 / 5 / 6 / 8
-// branches; this rule picks 4.
+// Branches of the graph: batch_branch_rule (batch_rule.h) over the plans'
+// input + output bytes and this device's L2 size.
 static int branch_count(const Batch* B) {
   const int n = (int)B->plans.size();
   double total = 0;
@@ -62,11 +58,7 @@ static int branch_count(const Batch* B) {
     cudaGetLastError();
     l2 = 0;
   }
-  int k = kBatchStreams;
-  if (n > 0 && total > 0 && l2 > 0) k = (int)(0.8 * (double)l2 / (total / n));
-  if (k < 2) k = 2;
-  if (k > kBatchStreams) k = kBatchStreams;
-  return k < n ? k : n;
+  return batch_branch_rule(n, total, l2, kBatchStreams);
 }
 
 // Records the batch into a graph on the batch's own capture stream (nothing

@@ -22,8 +22,15 @@
 //    reads, so nothing needs clearing.  Calls whose kernels overlap on the
 //    GPU (two streams, two threads) race on it: serialise them.
 //  * The first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress (with that device current); make that first call
-//    before any stream capture.
+//    cudaGetSymbolAddress (with that device current).  With CUDA's lazy
+//    module loading that lookup is also when the library's device code is
+//    loaded on that device and the 16 MiB array is reserved, so the first
+//    call itself does allocate: make it once at start-up (a tiny ndim = 1
+//    call will do), before the caller's memory pool has grown to fill the
+//    GPU and before any stream capture.
+//  * Every length is checked (13-smooth, stage count, one CTA, shared
+//    memory) before anything is launched, so a rejected call leaves the
+//    stream and the array untouched.
 #include <mutex>
 #include "dfft.h"
 #include "dfft_internal.h"
@@ -61,20 +68,31 @@ cudaError_t noalloc_setup(int dev, float2** out) {
   return cudaSuccess;
 }
 
-// Radices of the dynamic kernel, without allocating (16/8/4/2, 13/11/7/5/3).
+// Radices of the dynamic kernel, without allocating (16/8/4/2, 13/11/7/5/3),
+// at most kMaxStages of them.  Returns the stage count, 0 when L has a prime
+// factor above 13, -1 when it needs more than kMaxStages stages.
 int radices(int L, int* r) {
   int n = L, k = 0;
+  auto put = [&](int x) {
+    if (k >= kMaxStages) return false;
+    r[k++] = x;
+    return true;
+  };
   const int odd[] = {13, 11, 7, 5, 3};
   for (int p : odd)
-    while (n % p == 0) { r[k++] = p; n /= p; }
+    while (n % p == 0) {
+      if (!put(p)) return -1;
+      n /= p;
+    }
   int e = 0;
   while (n % 2 == 0) { ++e; n /= 2; }
   if (n != 1) return 0;
-  while (e >= 4) { r[k++] = 16; e -= 4; }
-  if (e == 3) r[k++] = 8;
-  if (e == 2) r[k++] = 4;
-  if (e == 1) r[k++] = 2;
-  if (k == 0) r[k++] = 1;
+  for (; e >= 4; e -= 4)
+    if (!put(16)) return -1;
+  if (e == 3 && !put(8)) return -1;
+  if (e == 2 && !put(4)) return -1;
+  if (e == 1 && !put(2)) return -1;
+  if (k == 0) put(1);
   return k;
 }
 
@@ -87,13 +105,26 @@ IoAny side(int kind, long long I, long long extent) {
   return x;
 }
 
-// Launch one pass of the computed-twiddle dynamic kernel.
-int launch(int L, long long I, long long O, double scale, IoAny in, IoAny out, cudaStream_t st) {
-  PassDesc d{};
+// One pass of the computed-twiddle dynamic kernel: descriptor, CTA shape and
+// shared memory, or an error for a length it cannot run (nothing launched).
+struct NaPass {
+  PassDesc d;
+  int C;
+  size_t col;
+};
+
+int prepare(int L, long long I, long long O, double scale, NaPass* np) {
+  PassDesc& d = np->d;
+  d = PassDesc{};
   int rad[kMaxStages];
   const int nst = radices(L, rad);
   if (nst == 0) {
     set_error("irfft_noalloc: length " + std::to_string(L) + " has a prime factor above 13");
+    return DFFT_ERROR_UNSUPPORTED_SIZE;
+  }
+  if (nst < 0) {
+    set_error("irfft_noalloc: length " + std::to_string(L) + " needs more than " +
+              std::to_string(kMaxStages) + " radix stages");
     return DFFT_ERROR_UNSUPPORTED_SIZE;
   }
   d.L = L;
@@ -121,8 +152,6 @@ int launch(int L, long long I, long long O, double scale, IoAny in, IoAny out, c
   d.scale = scale;
   d.Q = I * O;
   d.I = I;
-  d.in = in;
-  d.out = out;
   const size_t col = (size_t)ld * sizeof(float2);
   if (col > 200 * 1024) {
     set_error("irfft_noalloc: length " + std::to_string(L) + " does not fit shared memory");
@@ -138,10 +167,19 @@ int launch(int L, long long I, long long O, double scale, IoAny in, IoAny out, c
   }
   while (C > 1 && (C * P > 1024 || (size_t)C * col > 200 * 1024)) C /= 2;
   d.C = C;
-  const long long nblk = (d.Q + C - 1) / C;
-  void* args[] = {&d};
+  np->C = C;
+  np->col = col;
+  return DFFT_SUCCESS;
+}
+
+int launch(NaPass& np, IoAny in, IoAny out, cudaStream_t st) {
+  np.d.in = in;
+  np.d.out = out;
+  const long long nblk = (np.d.Q + np.C - 1) / np.C;
+  void* args[] = {&np.d};
   cudaError_t e = cudaLaunchKernel(reinterpret_cast<const void*>(&axis_pass_dynamic<float, 16, true>),
-                                   dim3((unsigned)nblk), dim3((unsigned)(C * P)), args, (size_t)C * col, st);
+                                   dim3((unsigned)nblk), dim3((unsigned)(np.C * np.d.P)), args,
+                                   (size_t)np.C * np.col, st);
   if (e != cudaSuccess) {
     set_error(std::string("irfft_noalloc: launch failed: ") + cudaGetErrorString(e));
     return DFFT_ERROR_CUDA;
@@ -175,6 +213,22 @@ extern "C" int dfft_irfft_noalloc_f32(const void* in, void* out, int ndim, const
               " complex elements; the static workspace holds at most " + std::to_string(kNoAllocElems));
     return DFFT_ERROR_INVALID_VALUE;
   }
+  // every pass is checked before the device is touched or anything launched
+  const long long O1 = H[1] * H[2];
+  const bool even = d % 2 == 0;
+  const int L1 = even ? (int)(d / 2) : (int)d;
+  NaPass passes[3];
+  for (int a = ndim - 1; a >= 1; --a) {
+    long long I = 1, O = 1;
+    for (int k = 0; k < a; ++k) I *= H[k];
+    for (int k = a + 1; k < 3; ++k) O *= H[k];
+    const int stt = prepare((int)H[a], I, O, 1.0 / (double)H[a], &passes[a]);
+    if (stt) return stt;
+  }
+  {
+    const int stt = prepare(L1, 1, O1, 1.0 / (double)d, &passes[0]);
+    if (stt) return stt;
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     set_error("irfft_noalloc: no usable current device");
@@ -191,28 +245,23 @@ extern "C" int dfft_irfft_noalloc_f32(const void* in, void* out, int ndim, const
   // the first into the static workspace, the rest in place there
   const void* src = in;
   for (int a = ndim - 1; a >= 1; --a) {
-    long long I = 1, O = 1;
+    long long I = 1;
     for (int k = 0; k < a; ++k) I *= H[k];
-    for (int k = a + 1; k < 3; ++k) O *= H[k];
     IoAny i = side(IO_CPLX, I, H[a]);
     IoAny o = side(IO_CPLX, I, H[a]);
     i.p = const_cast<void*>(src);
     o.p = scratch;
-    int stt = launch((int)H[a], I, O, 1.0 / (double)H[a], i, o, st);
+    const int stt = launch(passes[a], i, o, st);
     if (stt) return stt;
     src = scratch;
   }
   // C2R along dim 1
-  const long long O = H[1] * H[2];
   IoAny i, o;
-  int L;
-  if (d % 2 == 0) {
-    L = (int)(d / 2);
+  if (even) {
     i = side(IO_HERM_PAIR, 1, H[0]);
-    i.n = L;
+    i.n = L1;
     o = side(IO_REAL_PAIR, 1, d);
   } else {
-    L = (int)d;
     i = side(IO_HERM_FULL, 1, H[0]);
     i.n = (int)d;
     o = side(IO_REAL, 1, d);
@@ -220,5 +269,5 @@ extern "C" int dfft_irfft_noalloc_f32(const void* in, void* out, int ndim, const
   i.p = const_cast<void*>(src);
   i.w = nullptr;  // twiddles computed in the kernel
   o.p = out;
-  return launch(L, 1, O, 1.0 / (double)d, i, o, st);
+  return launch(passes[0], i, o, st);
 }

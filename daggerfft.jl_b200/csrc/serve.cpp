@@ -15,9 +15,20 @@
 // on the device; requests that arrive while others run join as soon as a
 // slot and memory free up.
 //
-// Latency = completion time - submit time (host steady clock).  Every wait
-// is bounded (DFFT_ERROR_TIMEOUT), queued requests can be cancelled, and a
-// request that can never fit the budget is rejected at submit.
+// Latency = completion time - submit time (host steady clock); the submit
+// time is taken on entry to dfft_server_submit, so the build of a plan for a
+// shape the server has not seen yet counts in that request's latency.  Plans
+// are built outside the server mutex (one build at a time), so a cold shape
+// never holds up admission or retirement of the requests already in flight.
+// Every wait is bounded (DFFT_ERROR_TIMEOUT), queued requests can be
+// cancelled, and a request that can never fit the budget is rejected at
+// submit.
+//
+// Admission is in arrival order, with one bounded exception: when the
+// request at the head of the queue is waiting for arena memory, up to
+// `slots` later requests that fit may start before it (each of them
+// finishes and frees its memory; after that many the head is served
+// strictly first), so one large request does not idle the slots behind it.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -144,7 +155,13 @@ struct Server {
   Arena arena;
   std::vector<std::unique_ptr<Slot>> slots;
   std::mutex mu;
-  std::condition_variable cv;       // dispatcher wake-up
+  // dispatcher wake-up: a flag under its own mutex, which is never held
+  // across a CUDA call, so the completion callback may take it (a wake-up
+  // sent between the dispatcher's last check and its wait is not lost)
+  std::mutex wake_mu;
+  std::condition_variable wake_cv;
+  bool wake = false;
+  std::mutex build_mu;              // plan builds, one at a time, outside `mu`
   std::condition_variable done_cv;  // waiters
   std::deque<Req*> queue;
   std::unordered_map<uint64_t, Req*> reqs;
@@ -153,6 +170,7 @@ struct Server {
   std::map<PlanKey, Plan*> shared_plans;      // one resident plan per shape
   std::vector<Plan*> all_plans;
   uint64_t next_id = 1;
+  int head_bypassed = 0;            // later requests admitted past a blocked head
   bool stop = false;
   std::thread thr;
   Clock::time_point t0;
@@ -161,6 +179,13 @@ struct Server {
   size_t peak_used = 0;
   int peak_running = 0;
   ~Server();
+  void poke() {
+    {
+      std::lock_guard<std::mutex> g(wake_mu);
+      wake = true;
+    }
+    wake_cv.notify_all();
+  }
 };
 
 // Host callback at the end of a request's stream work: no CUDA calls and no
@@ -169,33 +194,77 @@ static void CUDART_CB on_done(void* p) {
   Slot* s = static_cast<Slot*>(p);
   s->t_done_ns.store(Clock::now().time_since_epoch().count(), std::memory_order_relaxed);
   s->done.store(1, std::memory_order_release);
-  s->srv->cv.notify_all();
+  s->srv->poke();
 }
 
 // Server plans own no workspace (kFlagCallerWorkspace): while it runs a
 // plan only reads its tables, and each request brings its workspace (C2R
 // scratch, Bluestein scratch, fused-pass counters) from the arena, so one
-// resident instance serves every concurrent request of its shape.
+// resident instance serves every concurrent request of its shape.  Called
+// without `mu` held: the build (device allocations, twiddle uploads, tuning
+// launches) runs under build_mu only.
 static Plan* get_plan(Server* S, const PlanKey& k, const dfft_request& r) {
-  auto sh = S->shared_plans.find(k);
-  if (sh != S->shared_plans.end()) return sh->second;
-  Plan* p = build_plan(r.ndim, r.shape, r.precision, r.transform, r.ndims, r.dims, r.r2r_kinds, r.irfft_len,
-                       r.decomp, DFFT_PLAIN, (S->flags & DFFT_FLAG_TUNE) | kFlagCallerWorkspace);
-  S->all_plans.push_back(p);
-  S->shared_plans[k] = p;
-  return p;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto sh = S->shared_plans.find(k);
+    if (sh != S->shared_plans.end()) return sh->second;
+  }
+  std::lock_guard<std::mutex> bl(S->build_mu);
+  {
+    std::lock_guard<std::mutex> lk(S->mu);  // built by another thread meanwhile?
+    auto sh = S->shared_plans.find(k);
+    if (sh != S->shared_plans.end()) return sh->second;
+  }
+  std::unique_ptr<Plan> p(build_plan(r.ndim, r.shape, r.precision, r.transform, r.ndims, r.dims, r.r2r_kinds,
+                                     r.irfft_len, r.decomp, DFFT_PLAIN,
+                                     (S->flags & DFFT_FLAG_TUNE) | kFlagCallerWorkspace));
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->all_plans.push_back(p.get());
+  S->shared_plans[k] = p.get();
+  return p.release();
 }
 
 static size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// Admit queued requests in order while a slot and arena memory are free.
+// Takes the arena memory request q needs; false (nothing taken) if it does
+// not fit now.
+static bool reserve(Server* S, Req* q, size_t* oin, size_t* oout, size_t* owork, bool* gin, bool* gout,
+                    bool* gwork) {
+  *gin = *gout = *gwork = false;
+  if (q->r.in_location == DFFT_MEM_HOST) {
+    if (!S->arena.alloc(q->in_bytes, oin)) return false;
+    *gin = true;
+  }
+  if (q->r.out_location != DFFT_MEM_DEVICE) {
+    if (!S->arena.alloc(q->out_bytes, oout)) {
+      if (*gin) S->arena.release(*oin);
+      *gin = false;
+      return false;
+    }
+    *gout = true;
+  }
+  if (q->work_bytes + q->chirp_bytes) {
+    if (!S->arena.alloc(round256(q->work_bytes) + q->chirp_bytes, owork)) {
+      if (*gin) S->arena.release(*oin);
+      if (*gout) S->arena.release(*oout);
+      *gin = *gout = false;
+      return false;
+    }
+    *gwork = true;
+  }
+  return true;
+}
+
+// Admit queued requests in order while a slot and arena memory are free;
+// while the head waits for memory, at most `slots` later requests that fit
+// go past it (head_bypassed counts them; it resets when the head starts).
 static void admit(Server* S, std::unique_lock<std::mutex>& lk) {
   while (!S->queue.empty()) {
-    Req* q = S->queue.front();
-    if (q->state == 3) {  // cancelled while queued
+    while (!S->queue.empty() && S->queue.front()->state == 3) {  // cancelled while queued
       S->queue.pop_front();
-      continue;
+      S->head_bypassed = 0;
     }
+    if (S->queue.empty()) return;
     int free_slot = -1;
     for (auto& s : S->slots)
       if (!s->req) {
@@ -203,30 +272,20 @@ static void admit(Server* S, std::unique_lock<std::mutex>& lk) {
         break;
       }
     if (free_slot < 0) return;
-    size_t oin = 0, oout = 0;
-    bool gin = false, gout = false;
-    if (q->r.in_location == DFFT_MEM_HOST) {
-      if (!S->arena.alloc(q->in_bytes, &oin)) return;
-      gin = true;
+    size_t oin = 0, oout = 0, owork = 0;
+    bool gin = false, gout = false, gwork = false;
+    auto pick = S->queue.begin();
+    if (reserve(S, *pick, &oin, &oout, &owork, &gin, &gout, &gwork)) {
+      S->head_bypassed = 0;
+    } else {
+      if (S->head_bypassed >= (int)S->slots.size()) return;
+      for (++pick; pick != S->queue.end(); ++pick)
+        if ((*pick)->state != 3 && reserve(S, *pick, &oin, &oout, &owork, &gin, &gout, &gwork)) break;
+      if (pick == S->queue.end()) return;
+      S->head_bypassed++;
     }
-    if (q->r.out_location != DFFT_MEM_DEVICE) {
-      if (!S->arena.alloc(q->out_bytes, &oout)) {
-        if (gin) S->arena.release(oin);
-        return;
-      }
-      gout = true;
-    }
-    size_t owork = 0;
-    bool gwork = false;
-    if (q->work_bytes + q->chirp_bytes) {
-      if (!S->arena.alloc(round256(q->work_bytes) + q->chirp_bytes, &owork)) {
-        if (gin) S->arena.release(oin);
-        if (gout) S->arena.release(oout);
-        return;
-      }
-      gwork = true;
-    }
-    S->queue.pop_front();
+    Req* q = *pick;
+    S->queue.erase(pick);
     q->off_in = oin;
     q->off_out = oout;
     q->off_work = owork;
@@ -243,13 +302,7 @@ static void admit(Server* S, std::unique_lock<std::mutex>& lk) {
     int running = 0;
     for (auto& s : S->slots) running += s->req ? 1 : 0;
     S->peak_running = std::max(S->peak_running, running);
-    int st = DFFT_SUCCESS;
-    try {
-      q->plan = get_plan(S, q->key, q->r);
-    } catch (const Error& e) {
-      st = e.status;
-      set_error(e.msg);
-    }
+    int st = DFFT_SUCCESS;  // q->plan was built (or found) at submit
     // enqueue outside the lock: the stream work does not touch server state
     lk.unlock();
     if (st == DFFT_SUCCESS) {
@@ -306,7 +359,6 @@ static void retire(Server* S) {
       S->arena.release(q->off_work);
       q->has_work = false;
     }
-    q->plan = nullptr;
     if (q->state == 2) {
       S->n_done++;
       S->bytes_done += (double)(q->in_bytes + q->out_bytes);
@@ -326,7 +378,13 @@ static void dispatcher(Server* S) {
     retire(S);
     admit(S, lk);
     retire(S);
-    S->cv.wait_for(lk, std::chrono::milliseconds(5));
+    lk.unlock();
+    {
+      std::unique_lock<std::mutex> wl(S->wake_mu);
+      S->wake_cv.wait_for(wl, std::chrono::milliseconds(5), [S] { return S->wake; });
+      S->wake = false;
+    }
+    lk.lock();
   }
 }
 
@@ -335,7 +393,7 @@ Server::~Server() {
     std::lock_guard<std::mutex> lk(mu);
     stop = true;
   }
-  cv.notify_all();
+  poke();
   if (thr.joinable()) thr.join();
   for (auto& s : slots)
     if (s && s->stream) {
@@ -426,10 +484,12 @@ int dfft_server_submit(dfft_server server, const dfft_request* req, uint64_t* id
       k.kinds[i] = req->transform == DFFT_R2R ? req->r2r_kinds[i] : 0;
     }
     q->key = k;
+    q->t_submit = dfft::Clock::now();
     // the plan is built (or taken from the resident cache) at submit, so
-    // admission only moves data
-    std::unique_lock<std::mutex> lk(S->mu);
+    // admission only moves data; a build runs without the server mutex
     dfft::Plan* p = dfft::get_plan(S, k, *req);
+    q->plan = p;
+    std::unique_lock<std::mutex> lk(S->mu);
     q->in_bytes = p->in_bytes();
     q->out_bytes = p->out_bytes();
     q->work_bytes = p->work_bytes;
@@ -444,13 +504,12 @@ int dfft_server_submit(dfft_server server, const dfft_request* req, uint64_t* id
                                                 " staging bytes, more than the server's HBM budget"};
     }
     q->id = S->next_id++;
-    q->t_submit = dfft::Clock::now();
     *id = q->id;
     dfft::Req* raw = q.release();
     S->reqs[raw->id] = raw;
     S->queue.push_back(raw);
     lk.unlock();
-    S->cv.notify_all();
+    S->poke();
   });
 }
 
@@ -537,7 +596,7 @@ int dfft_server_release(dfft_server server, uint64_t id) {
       S->reqs.erase(it);
       delete q;
     }
-    S->cv.notify_all();
+    S->poke();
   });
 }
 

@@ -278,7 +278,13 @@ DFFT_API int dfft_copy_plan_destroy(dfft_copy_plan plan);
  * device array of 2^21 ComplexF32 (16 MiB) that every GPU loading the
  * library keeps until exit; larger sizes return DFFT_ERROR_INVALID_VALUE.
  * Calls that overlap on the GPU race on that array.  The first call on a
- * device looks up the array's address; make it before any stream capture.
+ * device looks up the array's address, which (CUDA loads modules lazily) is
+ * also when the library's device code and the 16 MiB array are loaded on that
+ * device: make one small call (ndim = 1 will do) at start-up, before the
+ * caller's pool has grown to fill the GPU and before any stream capture.
+ * Every length is checked before anything is launched (13-smooth, at most 16
+ * radix stages, one CTA per pencil); rejected lengths return
+ * DFFT_ERROR_UNSUPPORTED_SIZE and leave the stream untouched.
  * in: (shape[0]/2+1, shape[1], shape[2]) ComplexF32, out: shape Float32,
  * both column-major device memory.
  */

@@ -65,3 +65,16 @@ def test_gpu_arm_line():
     assert e2e["results_consistent"] is True
     assert d["gpu_launches"] == 4 * d["steps"]  # fused slab + dim-3 pass, forward and inverse
     assert "sm_mhz" in d["clocks"] and "reasons" in d["clocks"]
+    er = d["errors"]
+    assert er["fwd_rel_l2_vs_host_fp64"] <= 1e-5 and er["inv_rel_l2_vs_host_fp64"] <= 1e-5
+    assert er["roundtrip_rel_l2"] <= 1e-5
+    cf = d["configs"]
+    for k in ("c1", "c2", "c4", "c5"):
+        assert "error" not in cf[k], cf[k]
+    assert cf["c1"]["fwd_rel_l2_vs_host_fp64"] <= 1e-12 and cf["c1"]["roundtrip_rel_l2"] <= 1e-12
+    for r in cf["c2"]["results"]:
+        tol = 1e-12 if r["precision"] == "Float64" else 1e-5
+        assert r["fwd_rel_l2_vs_host_fp64"] <= tol and r["inv_rel_l2_vs_host_fp64"] <= tol
+    assert cf["c4"]["grids_worst_fwd_rel_l2_vs_host_fp64"] <= 1e-5
+    assert cf["c4"]["dct2_rel_l2_vs_host_fp64"] <= 1e-12 and cf["c4"]["dct3_rel_l2_vs_host_fp64"] <= 1e-12
+    assert all(r["completed"] > 0 and r["p99_ms"] > 0 for r in cf["c5"]["rates"])

@@ -61,3 +61,35 @@ def test_python_tags_mirror_reference():
     assert dfft.Pencil() == dfft.Pencil() and dfft.Pencil() != dfft.Slab()
     with pytest.raises(dfft.ArgumentError, match="Unknown transform type"):
         dfft.R2R((99,))
+
+
+def _noalloc_status(shape):
+    """dfft_irfft_noalloc_f32 with placeholder pointers: every length check
+    runs before the device is touched, so a rejected shape returns its
+    status here without a GPU (the pointers are never dereferenced)."""
+    import dfft
+    from dfft import _lib
+    L = dfft.lib()
+    L.dfft_irfft_noalloc_f32.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p]
+    L.dfft_irfft_noalloc_f32.restype = ctypes.c_int
+    return L.dfft_irfft_noalloc_f32(ctypes.c_void_p(256), ctypes.c_void_p(512), len(shape),
+                                    _lib.i64_array(shape), None)
+
+
+@pytest.mark.parametrize("shape", [(2 * 3 ** 17,), (3 ** 17,), (3 ** 18,)])
+def test_noalloc_rejects_too_many_stages_without_gpu(shape):
+    from dfft import _lib
+    import dfft
+    assert _noalloc_status(shape) == _lib.ERROR_UNSUPPORTED_SIZE
+    assert b"radix stages" in dfft.lib().dfft_last_error()
+
+
+@pytest.mark.parametrize("shape", [(16, 17, 2), (16, 4, 34), (2 * 17,)])
+def test_noalloc_checks_every_axis_before_launch(shape):
+    # a prime factor above 13 on any axis (dims 2 and 3 run first) is
+    # rejected before the first pass is queued
+    from dfft import _lib
+    import dfft
+    assert _noalloc_status(shape) == _lib.ERROR_UNSUPPORTED_SIZE
+    assert b"prime factor above 13" in dfft.lib().dfft_last_error()
