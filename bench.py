@@ -28,6 +28,11 @@ errors : relative L2 of the forward result against a float64 host fftn
          (scipy.fft on all host cores) of the same input, of the inverse
          result against the host ifftn of the GPU's forward output, and of
          the round trip against the input.
+mixed  : the same step in the mixed (tensor-core) form -- the 512-point
+         axes as radix-32 x radix-16 complex matrix products on tcgen05
+         with FP16 hi+lo split operands and FP32 accumulation -- timed the
+         same way, with its per-launch times, its ratio to the plain step
+         and its errors against the float64 host evaluation.
 configs: (one GPU) the other configured workloads, each with its time,
          algorithmic GB/s and errors against a float64 host evaluation:
          c1 128^3 ComplexF64 Pencil, c2 256^3 Float64/Float32 rfft+irfft,
@@ -219,6 +224,62 @@ def host_errors(A_host, Fd, Bd):
             "host_oracle": f"scipy.fft float64, {w} threads"}
 
 
+def run_mixed(args, dfft, decomp, Ad, Bd, Cd, stream, plain_ms, A_host):
+    """The step in the mixed form: fwd + inv through method="mixed" plans,
+    warm-up, then args.steps steps between CUDA events on the stream."""
+    import torch
+    try:
+        pf = dfft.get_or_create_gpu_plan(dfft.FFT(), Ad, (1, 2, 3), decomp=decomp, method="mixed")
+        pi = dfft.get_or_create_gpu_plan(dfft.IFFT(), Bd, (1, 2, 3), decomp=decomp, method="mixed")
+    except Exception as e:
+        return {"error": f"{type(e).__name__}: {e}"}
+
+    def step():
+        pf.execute(Ad, Bd, stream)
+        pi.execute(Bd, Cd, stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    out = {"ms_per_step": round(ms, 4), "value": round(STEP_BYTES / (ms * 1e-3) / 1e9, 2), "unit": "GB/s",
+           "speedup_vs_plain": round(plain_ms / ms, 4), "launches_per_step": pf.launches + pi.launches,
+           "kernels": pf.describe().strip().splitlines()}
+    # each forward launch alone (one pass per axis)
+    per = {}
+    for dims in ((1,), (2,), (3,)):
+        p = dfft.gpu_plan_transform(dfft.FFT(), Ad, dims, decomp=decomp, method="mixed")
+        for _ in range(3):
+            p.execute(Ad, Bd, stream)
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(10):
+            p.execute(Ad, Bd, stream)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        per[str(dims[0])] = round(a0.elapsed_time(a1) / 10, 4)
+        del p
+    out["per_launch_ms"] = per
+    peak, _ = measured_peak()
+    dom = max(per.values())
+    out["dominant_frac_of_peak"] = round(PASS_BYTES / (dom * 1e-3) / 1e9 / peak, 4)
+    if A_host is not None:
+        step()
+        torch.cuda.synchronize()
+        err = host_errors(A_host, Bd, Cd)
+        err["roundtrip_rel_l2"] = float(torch.linalg.vector_norm(Cd - Ad) / torch.linalg.vector_norm(Ad))
+        out["errors"] = err
+    return out
+
+
 def run_configs():
     import bench_configs as bc
     out = {}
@@ -284,6 +345,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--method", default="plain", choices=["plain", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed (tensor-core) form of the step")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other configured workloads (c1, c2, c4, c5)")
     ap.add_argument("--no-tune", action="store_true", help="heuristic launch shapes, no autotuning")
@@ -378,6 +441,11 @@ def main():
     rt = float(torch.linalg.vector_norm(Cd - Ad) / torch.linalg.vector_norm(Ad))
     errors = host_errors(A_host, Bd, Cd) if rank == 0 else {}
     errors["roundtrip_rel_l2"] = rt
+
+    # the mixed (tensor-core) form of the same step, unless it is the headline
+    mixed = None
+    if args.method == "plain" and not args.no_mixed:
+        mixed = run_mixed(args, dfft, decomp, Ad, Bd, Cd, stream, t_ms, A_host if rank == 0 else None)
 
     # the step's launches timed alone (roofline of the dominant one): the
     # forward plan is either the fused dims-(1,2) slab pass + the dim-3 pass,
@@ -531,6 +599,8 @@ def main():
             "errors": errors,
             "clocks": clk,
         }
+        if mixed is not None:
+            line["mixed"] = mixed
         if configs is not None:
             line["configs"] = configs
         print(json.dumps(line), flush=True)
