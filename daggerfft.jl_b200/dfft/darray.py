@@ -374,47 +374,54 @@ def _inplace(t):
     raise ArgumentError(_lib.ERROR_UNKNOWN_TRANSFORM, "Unknown transform type")
 
 
-def gpu_fft_(*args, group=None):
+def gpu_fft_(*args, group=None, stage=None, copier=None):
     """Pencil: ``gpu_fft!(C, A, B, wsAB, wsBC, transforms, dims, Pencil())``
     (src/fftgpu.jl:498-531); Slab: ``gpu_fft!(B, A, wsAB, transforms, dims,
     Slab())`` (src/fftgpu.jl:534-557).  The reference's ``scope`` argument
-    (a Dagger processor set) has no meaning on one GPU and is not taken."""
+    (a Dagger processor set) has no meaning on one GPU and is not taken.
+    ``stage(D, transform, dims)`` transforms the local chunks of D in place
+    (default: libdfft plans on each chunk) and ``copier`` runs the copy
+    phases of the redistributions (default: libdfft copy plans); both are
+    replaceable so that the exchange schedule runs on CPU ranks too."""
+    st = stage or _stage
     decomp = args[-1]
     if isinstance(decomp, Slab):
         B, A, wsAB, transforms, dims, _ = args
-        _stage(A, _inplace(transforms[0]), (dims[0], dims[1]))
-        gpu_coalesced_redistribute_(B, A, wsAB, 1, group)
-        _stage(B, _inplace(transforms[2]), (dims[2],))
+        st(A, _inplace(transforms[0]), (dims[0], dims[1]))
+        gpu_coalesced_redistribute_(B, A, wsAB, 1, group, copier)
+        st(B, _inplace(transforms[2]), (dims[2],))
         return B
     if isinstance(decomp, Pencil):
         C, A, B, wsAB, wsBC, transforms, dims, _ = args
-        _stage(A, _inplace(transforms[0]), (dims[0],))
-        gpu_coalesced_redistribute_(B, A, wsAB, 1, group)
-        _stage(B, _inplace(transforms[1]), (dims[1],))
-        gpu_coalesced_redistribute_(C, B, wsBC, 2, group)
-        _stage(C, _inplace(transforms[2]), (dims[2],))
+        st(A, _inplace(transforms[0]), (dims[0],))
+        gpu_coalesced_redistribute_(B, A, wsAB, 1, group, copier)
+        st(B, _inplace(transforms[1]), (dims[1],))
+        gpu_coalesced_redistribute_(C, B, wsBC, 2, group, copier)
+        st(C, _inplace(transforms[2]), (dims[2],))
         return C
     raise ArgumentError(_lib.ERROR_INVALID_VALUE, "last argument must be Pencil() or Slab()")
 
 
-def gpu_ifft_(*args, group=None):
+def gpu_ifft_(*args, group=None, stage=None, copier=None):
     """Pencil: ``gpu_ifft!(C, A, B, wsAB, wsBC, transforms, dims, Pencil())``
     (src/fftgpu.jl:560-593: transforms[3] on dims[3] first); Slab:
-    ``gpu_ifft!(A, B, wsBA, transforms, dims, Slab())`` (src/fftgpu.jl:596-619)."""
+    ``gpu_ifft!(A, B, wsBA, transforms, dims, Slab())`` (src/fftgpu.jl:596-619).
+    ``stage`` and ``copier`` as in ``gpu_fft_``."""
+    st = stage or _stage
     decomp = args[-1]
     if isinstance(decomp, Slab):
         A, B, wsBA, transforms, dims, _ = args
-        _stage(B, _inplace(transforms[2]), (dims[2],))
-        gpu_coalesced_redistribute_(A, B, wsBA, 3, group)
-        _stage(A, _inplace(transforms[0]), (dims[0], dims[1]))
+        st(B, _inplace(transforms[2]), (dims[2],))
+        gpu_coalesced_redistribute_(A, B, wsBA, 3, group, copier)
+        st(A, _inplace(transforms[0]), (dims[0], dims[1]))
         return A
     if isinstance(decomp, Pencil):
         C, A, B, wsAB, wsBC, transforms, dims, _ = args
-        _stage(A, _inplace(transforms[2]), (dims[2],))
-        gpu_coalesced_redistribute_(B, A, wsAB, 3, group)
-        _stage(B, _inplace(transforms[1]), (dims[1],))
-        gpu_coalesced_redistribute_(C, B, wsBC, 4, group)
-        _stage(C, _inplace(transforms[0]), (dims[0],))
+        st(A, _inplace(transforms[2]), (dims[2],))
+        gpu_coalesced_redistribute_(B, A, wsAB, 3, group, copier)
+        st(B, _inplace(transforms[1]), (dims[1],))
+        gpu_coalesced_redistribute_(C, B, wsBC, 4, group, copier)
+        st(C, _inplace(transforms[0]), (dims[0],))
         return C
     raise ArgumentError(_lib.ERROR_INVALID_VALUE, "last argument must be Pencil() or Slab()")
 
