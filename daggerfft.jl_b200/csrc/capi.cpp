@@ -77,13 +77,15 @@ int dfft_plan_describe(dfft_plan plan, char* buf, size_t len) {
     if (!buf || len == 0) throw Error{DFFT_ERROR_INVALID_VALUE, "buf is NULL or len is 0"};
     std::string out;
     for (const dfft::Pass& q : p->passes) {
-      const char* kind = q.slab ? "slab-xy" : q.feed ? "strided-feed" : q.async_ ? "strided-async"
+      const char* kind = q.mixed ? (q.mstrided ? "mixed-strided" : "mixed-contig")
+                         : q.slab ? "slab-xy" : q.feed ? "strided-feed" : q.async_ ? "strided-async"
                          : q.real ? "real-pipe"
                          : q.tiled == 1 ? "tiled-contig" : q.tiled == 2 ? "tiled-strided"
                          : q.pipe ? (q.tma ? "strided-pipe" : "contig-pipe")
                          : q.is_static ? "direct" : "dynamic";
       std::string rad;
       for (int i = 0; i < q.d.nst; ++i) rad += (i ? "x" : "") + std::to_string(q.d.radix[i]);
+      if (q.mixed) rad = "32x16(tcgen05 fp16 hi+lo)";
       char line[256];
       std::snprintf(line, sizeof line, "%s L=%d I=%lld O=%lld grid=%u block=%u smem=%zu radices=%s\n", kind,
                     q.d.L, q.d.I, q.d.I > 0 ? q.d.Q / q.d.I : 0LL, q.grid.x, q.block.x, q.smem,

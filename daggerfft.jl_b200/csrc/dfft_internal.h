@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 #include "async_pass.cuh"
+#include "mixed_pass.cuh"
 
 namespace dfft {
 
@@ -63,6 +64,9 @@ struct Pass {
   TiledGeom tgeom{};
   bool async_ = false;   // axis_pass_async (cp.async tiles, strides TMA cannot address)
   AsyncGeom ageom{};
+  bool mixed = false;    // mixed_pass (tensor-core radix-32 x 16 stages, L = 512 ComplexF32)
+  bool mstrided = false; // its strided variant (128-byte swizzled tensor maps {tI, tL, tO})
+  MixedGeom mgeom{};
   size_t ctr_bytes = 0;  // job and per-slab counters (in the plan workspace)
   PassDesc d2{};
   SlabGeom sgeom{};
@@ -111,6 +115,12 @@ Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v = 0);
 // variant under DFFT_FLAG_FUSE).
 int choose_slab(int dbl, int L, long long O, int inverse, const std::vector<Pass>& split,
                 unsigned flags);
+
+// Mixed (tensor-core) form: does mixed_pass serve this axis (ComplexF32,
+// L = 512, rows TMA can address), and the pass for it (one axis of Q = I*O
+// pencils; inverse scales by 1/512).
+bool mixed_supported(int dbl, int L, long long I);
+Pass make_mixed_pass(long long I, long long O, int inverse);
 
 // Device error word of the current device (bounded waits that expire set it).
 int* device_error_word();

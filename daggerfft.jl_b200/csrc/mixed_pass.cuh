@@ -1,0 +1,516 @@
+// Mixed-precision tensor-core axis pass for ComplexF32 length 512 (the
+// "mixed" arithmetic form): the 512-point DFT of every pencil runs as two
+// dense complex matrix products on the 5th-generation tensor cores,
+//
+//   n = 16*n1 + n2, k = k1 + 32*k2   (n1, k1 < 32; n2, k2 < 16)
+//   stage A: Y[n2, k1] = sum_n1 x[16 n1 + n2] W32^(n1 k1)       (radix 32)
+//   twiddle: Y'[n2, k1] = Y[n2, k1] W512^(n2 k1)                 (FP32, CUDA cores)
+//   stage B: X[k1 + 32 k2] = sum_n2 Y'[n2, k1] W16^(n2 k2)       (radix 16)
+//
+// Each product is a real GEMM over interleaved-free (re block, im block)
+// vectors: D[M = pencil rows][N = 2 x outputs] = A[M][K = 2 x inputs] B[K][N]
+// with B the real form [[Wr, Wi], [-Wi, Wr]] of the DFT matrix (K-major in
+// shared memory, FP64-generated).  Operands are FP16 hi + lo splits of FP32
+// values: D = A_hi B_hi + A_lo B_hi + A_hi B_lo, accumulated in FP32 in
+// tensor memory (the dropped A_lo B_lo term and the split residuals are
+// about 2^-22 of each value).  The tensor cores round each MMA's FP32
+// accumulation toward zero, so a long chain of K-steps into one accumulator
+// shrinks every result by a few ulps (a bias that adds up over passes: a
+// 12-step chain measured 1.75e-6 over a 4-pass round trip).  The products
+// therefore go to separate accumulators -- the hi x hi part in chains of at
+// most two K-steps, the two cross terms (about 2^-11 of it) in their own --
+// which the epilogue adds in FP32 with round-to-nearest.  (An n-step chain
+// shrinks the result, projected on itself, by about delta*(n+1)/2 with
+// delta = 0.36 * 2^-23 per rounding: 6.5 + 3.5 delta per pass for one chain
+// per stage, 1.5 + 1 delta with these splits.)  Before each split the values of one pencil
+// are scaled by a power of two so that the pencil's largest |re|, |im|
+// lies in [2^14, 2^15) (per-pencil scaling: FP16's range and the lo parts'
+// precision follow each pencil's own magnitude); the scale is undone
+// exactly after the product.  Twiddles and the inverse's 1/512 stay FP32 /
+// exact.
+//
+// Tile: 16 pencils (columns of a strided axis, or whole contiguous pencils)
+// x 512 points, 64 KB of ComplexF32.  Stage A is M = 256 rows (pencil c,
+// n2) x N = 64 x K = 64, two M = 128 MMAs per K-step; stage B is M = 512
+// rows (c, k1) x N = 32 x K = 32, four M = 128 MMAs per K-step.  TMEM (512
+// columns): stage A block h at 192 h (hi x hi K-steps 0-1 at +0, 2-3 at +64,
+// cross terms at +128); stage B block j at 96 j (hi x hi K-step 0 at +0,
+// K-step 1 at +32, cross terms at +64), reusing stage A's columns once its
+// epilogue has read them.
+//
+// Warp roles (320 threads, one CTA per SM, persistent over tiles):
+//   warps 0-7  convert / epilogue threads: thread t owns stage-A row t =
+//              (c = t/16, n2 = t%16) -- its prep (FP32 tile -> scaled FP16
+//              hi/lo, K-major 128B-swizzled rows), its TMEM row in the stage-A
+//              epilogue (unscale, twiddle, rescale, split into the stage-B
+//              operand, MN-major 128B-swizzled) -- and two stage-B rows
+//              (c, k1) in the final epilogue (unscale, store FP32).
+//   warp 8     producer: TMA / bulk loads into two tile buffers, TMA / bulk
+//              stores of finished tiles.
+//   warp 9     TMEM allocation; lane 0 issues the tcgen05.mma products and
+//              commits them to mbarriers.
+// Every mbarrier wait is bounded (~2 s) and also gives up when another role
+// has set the CTA's abort flag; on expiry the kernel records
+// DFFT_DEVERR_TMA_TIMEOUT, waits (bounded) for its copies and products in
+// flight, frees its tensor memory and returns.
+#pragma once
+#include <cuda_fp16.h>
+#include "tma_pass.cuh"
+
+namespace dfft {
+
+struct MixedGeom {
+  long long ntiles;   // tiles of 16 pencils
+  long long ncols;    // contiguous: pencils (the last tile may be partial)
+  int tiles_i;        // strided: tiles along the inner extent I
+  int lb, nlb;        // strided: rows per TMA box, boxes per tile
+  float out_scale;    // 1 (forward) or 1/512 (inverse), exact
+  const unsigned char* consts;  // operand images of the DFT matrices + twiddles (kMixConstBytes)
+  int* err;
+};
+
+// Shared-memory map (bytes from a 1024-byte aligned base).
+constexpr int kMixTile = 16 * 512 * 8;          // one FP32 complex tile (64 KB)
+constexpr int kMixOpA = 2 * kMixTile;           // operand hi (32 KB), lo at +32 KB
+constexpr int kMixOpBytes = 32768;
+constexpr int kMixB32 = kMixOpA + 2 * kMixOpBytes;  // DFT32 operand hi (8 KB), lo (8 KB)
+constexpr int kMixB16 = kMixB32 + 16384;            // DFT16 operand hi (4 KB), lo (4 KB)
+constexpr int kMixTw = kMixB16 + 8192;              // twiddles [n2][k1], rows of 33 (4224 B)
+constexpr int kMixConstBytes = kMixTw + 16 * 33 * 8 - kMixB32;
+constexpr int kMixMisc = kMixTw + 16 * 33 * 8;      // barriers, TMEM address, scales
+constexpr int kMixSmem = kMixMisc + 256 + 1024;     // + alignment slack
+constexpr int kMixThreads = 320;
+constexpr int kMixTmemCols = 512;
+
+// ---- tcgen05 wrappers -----------------------------------------------------
+
+// Shared-memory matrix descriptor: start address, leading / stride byte
+// offsets, descriptor version 1, 128-byte swizzle.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  const uint32_t lo = ((saddr & 0x3FFFFu) >> 4) | ((lbo >> 4) << 16);
+  const uint32_t hi = (sbo >> 4) | (1u << 14) | (2u << 29);
+  return ((uint64_t)hi << 32) | lo;
+}
+// Instruction descriptor of kind::f16 with FP16 A and B, FP32 D.
+__host__ __device__ constexpr uint32_t umma_idesc_f16(int M, int N, int a_mn_major, int b_mn_major) {
+  return (1u << 4) | ((uint32_t)a_mn_major << 15) | ((uint32_t)b_mn_major << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, int acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+#define DFFT_R8(i) "=r"(r[i]), "=r"(r[i + 1]), "=r"(r[i + 2]), "=r"(r[i + 3]), "=r"(r[i + 4]), \
+                   "=r"(r[i + 5]), "=r"(r[i + 6]), "=r"(r[i + 7])
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : DFFT_R8(0), DFFT_R8(8), DFFT_R8(16), DFFT_R8(24)
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,"
+      "%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+      : DFFT_R8(0), DFFT_R8(8), DFFT_R8(16), DFFT_R8(24), DFFT_R8(32), DFFT_R8(40), DFFT_R8(48), DFFT_R8(56)
+      : "r"(taddr));
+}
+#undef DFFT_R8
+
+// Power-of-two scale that puts a pencil maximum m in [2^14, 2^15) (clamped
+// to the normal range; m = 0 gives a harmless large scale).
+__device__ __forceinline__ float mix_scale(float m) {
+  int e = (int)((__float_as_uint(m) >> 23) & 0xFF);
+  int b = 268 - e;
+  b = b < 1 ? 1 : (b > 254 ? 254 : b);
+  return __uint_as_float((uint32_t)b << 23);
+}
+// FP16 hi / lo split of a pair of FP32 values (already scaled).
+__device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
+  const __half2 h = __floats2half2_rn(a, b);
+  const float2 f = __half22float2(h);
+  const __half2 l = __floats2half2_rn(a - f.x, b - f.y);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+__device__ __forceinline__ void sts128(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d)
+               : "memory");
+}
+__device__ __forceinline__ float2 lds64(uint32_t addr) {
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
+  return v;
+}
+__device__ __forceinline__ void sts64(uint32_t addr, float x, float y) {
+  asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(x), "f"(y) : "memory");
+}
+// Bounded mbarrier wait that also leaves when the CTA's abort flag is set.
+__device__ __forceinline__ bool mix_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (unsigned i = 1; i < kWaitLimit; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 255) == 0) {
+      if (*abort_flag) return false;
+      if (global_ns() - t0 > kWaitNs) return false;
+    }
+  }
+  return false;
+}
+// The same wait with a warp-uniform result (every lane waits; the warp
+// proceeds only if all lanes saw the phase complete), so that the
+// .sync.aligned tensor-memory loads after it run converged.
+__device__ __forceinline__ bool mix_wait_warp(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  const bool ok = mix_wait(bar, parity, abort_flag);
+  return __all_sync(0xffffffffu, ok) != 0;
+}
+
+// Byte offset of element (k, c) of a tile: strided tiles are [k][c] rows of
+// 16 complex (128 bytes) in TMA's 128-byte swizzle; contiguous tiles are
+// [c][k] pencils of 4 KB.
+template <bool STRIDED> __device__ __forceinline__ uint32_t tile_off(int k, int c) {
+  if constexpr (STRIDED) return (uint32_t)(k * 128 + ((((c >> 1) ^ (k & 7)) << 4) | ((c & 1) << 3)));
+  else return (uint32_t)(c * 4096 + k * 8);
+}
+
+// STRIDED: the axis has element stride I > 1 (tile = 16 adjacent columns,
+// TMA boxes {16, lb, 1} of the tensor {I, 512, O}); otherwise the axis is
+// contiguous (tile = 16 whole pencils, one bulk copy).  DIR: 1 forward, 2
+// inverse (selects the DFT matrices and twiddles in `consts`).
+template <bool STRIDED>
+__global__ void __launch_bounds__(kMixThreads, 1)
+    mixed_pass(const void* in, void* out, const __grid_constant__ CUtensorMap tin,
+               const __grid_constant__ CUtensorMap tout, const MixedGeom g) {
+  extern __shared__ __align__(1024) unsigned char smem_mix_raw[];
+  const uint32_t raw = smem_u32(smem_mix_raw);
+  const uint32_t pad = ((raw + 1023u) & ~1023u) - raw;
+  unsigned char* sm = smem_mix_raw + pad;
+  const uint32_t sb = raw + pad;  // aligned base (shared address)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kMixMisc);
+  uint64_t* full = bars;        // [2] tile loaded
+  uint64_t* outrdy = bars + 2;  // [2] tile transformed
+  uint64_t* opA = bars + 4;     // stage-A operands written
+  uint64_t* opB = bars + 5;     // stage-B operands written
+  uint64_t* accA = bars + 6;    // stage-A products done
+  uint64_t* accB = bars + 7;    // stage-B products done
+  uint64_t* scl = bars + 8;     // stage-B pencil scales written
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + kMixMisc + 96);
+  volatile int* s_abort = reinterpret_cast<volatile int*>(sm + kMixMisc + 100);
+  float* s_scaleB = reinterpret_cast<float*>(sm + kMixMisc + 128);  // [16]
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  volatile int* verr = g.err;
+
+  if (tid == 0) {
+    // full, accA, accB: one arrival (expect_tx / tcgen05.commit); outrdy,
+    // opA, opB, scl: one arrival per convert warp
+    for (int i = 0; i < 9; ++i) mbar_init(&bars[i], (i == 0 || i == 1 || i == 6 || i == 7) ? 1 : 8);
+    mbar_fence_init();
+    *s_abort = 0;
+  }
+  // constants: DFT operand images and the twiddle table
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(g.consts);
+    uint4* dst = reinterpret_cast<uint4*>(sm + kMixB32);
+    for (int i = tid; i < kMixConstBytes / 16; i += kMixThreads) dst[i] = src[i];
+  }
+  if (warp == 9) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_tmem)),
+                 "r"(kMixTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_proxy_async_smem();  // constants (generic writes) are read by the tensor cores
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+
+  const long long first = blockIdx.x, step = gridDim.x;
+
+  if (warp < 8) {
+    // ---------------- convert / epilogue threads ----------------
+    const int c = tid >> 4, n2 = tid & 15;
+    const int q = warp & 3;
+    const uint32_t opHi = sb + kMixOpA, opLo = opHi + kMixOpBytes;
+    const uint32_t twb = sb + kMixTw;
+    int it = 0;
+    for (long long tile = first; tile < g.ntiles; tile += step, ++it) {
+      const int b = it & 1;
+      if (!mix_wait_warp(&full[b], (uint32_t)((it >> 1) & 1), s_abort)) { *s_abort = 1; break; }
+      const uint32_t tb = sb + (uint32_t)b * kMixTile;
+      // ---- stage-A operands: row t = (c, n2), K = [re n1 0..31 | im n1 0..31]
+      float2 v[32];
+#pragma unroll
+      for (int n1 = 0; n1 < 32; ++n1) v[n1] = lds64(tb + tile_off<STRIDED>(16 * n1 + n2, c));
+      float m = 0.f;
+#pragma unroll
+      for (int n1 = 0; n1 < 32; ++n1) m = fmaxf(m, fmaxf(fabsf(v[n1].x), fabsf(v[n1].y)));
+#pragma unroll
+      for (int o = 8; o >= 1; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+      const float sA = mix_scale(m);
+      {
+        const uint32_t row = (uint32_t)tid * 128u;
+        const int r8 = tid & 7;
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          uint32_t h[4], l[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int n1 = 8 * (jj & 3) + 2 * e;
+            const float a0 = (jj < 4 ? v[n1].x : v[n1].y) * sA;
+            const float a1 = (jj < 4 ? v[n1 + 1].x : v[n1 + 1].y) * sA;
+            split2(a0, a1, h[e], l[e]);
+          }
+          const uint32_t off = row + (uint32_t)(((jj ^ r8) << 4));
+          sts128(opHi + off, h[0], h[1], h[2], h[3]);
+          sts128(opLo + off, l[0], l[1], l[2], l[3]);
+        }
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(opA);
+      // ---- stage-A epilogue: TMEM row t -> unscale, twiddle, rescale, split
+      if (!mix_wait_warp(accA, (uint32_t)(it & 1), s_abort)) { *s_abort = 1; break; }
+      tc_fence_after();
+      uint32_t r[64];
+      {
+        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((warp >> 2) * 192);
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {  // real parts (columns 0-31), then imaginary
+          uint32_t t0[32], t1[32];
+          tmem_ld32(ta + (uint32_t)(32 * part), t0);
+          tmem_ld32(ta + 64u + (uint32_t)(32 * part), t1);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 32; ++i) r[32 * part + i] = __float_as_uint(__uint_as_float(t0[i]) + __uint_as_float(t1[i]));
+          tmem_ld32(ta + 128u + (uint32_t)(32 * part), t0);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 32; ++i) r[32 * part + i] = __float_as_uint(__uint_as_float(r[32 * part + i]) + __uint_as_float(t0[i]));
+        }
+      }
+      const float iA = 1.0f / sA;  // exact: a power of two
+      float mb = 0.f;
+#pragma unroll
+      for (int k1 = 0; k1 < 32; ++k1) {
+        const float2 w = lds64(twb + (uint32_t)((n2 * 33 + k1) * 8));
+        const float yr = __uint_as_float(r[k1]) * iA, yi = __uint_as_float(r[32 + k1]) * iA;
+        const float zr = yr * w.x - yi * w.y, zi = yr * w.y + yi * w.x;
+        r[k1] = __float_as_uint(zr);
+        r[32 + k1] = __float_as_uint(zi);
+        mb = fmaxf(mb, fmaxf(fabsf(zr), fabsf(zi)));
+      }
+#pragma unroll
+      for (int o = 8; o >= 1; o >>= 1) mb = fmaxf(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+      const float sB = mix_scale(mb);
+      if (n2 == 0) s_scaleB[c] = sB;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(scl);
+      tc_fence_before();
+      {
+        // stage-B operand, MN-major: M = c*32 + k1 (atoms of 64 rows, 4 KB
+        // apart), K = [re n2 0..15 | im n2 0..15] (groups of 8 rows, 1 KB apart)
+        const int kr = n2 & 7;
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+          const uint32_t kbase = (uint32_t)((c >> 1) * 4096 + (2 * part + (n2 >> 3)) * 1024 + kr * 128);
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            uint32_t h[4], l[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int k1 = 8 * jj + 2 * e;
+              split2(__uint_as_float(r[32 * part + k1]) * sB, __uint_as_float(r[32 * part + k1 + 1]) * sB, h[e],
+                     l[e]);
+            }
+            const uint32_t off = kbase + (uint32_t)(((((c & 1) * 4 + jj) ^ kr) << 4));
+            sts128(opHi + off, h[0], h[1], h[2], h[3]);
+            sts128(opLo + off, l[0], l[1], l[2], l[3]);
+          }
+        }
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(opB);
+      // ---- stage-B epilogue: rows (c' = 4j + q, k1 = lane), j = 2*(warp/4) + jb
+      if (!mix_wait_warp(accB, (uint32_t)(it & 1), s_abort) || !mix_wait_warp(scl, (uint32_t)(it & 1), s_abort)) {
+        *s_abort = 1;
+        break;
+      }
+      tc_fence_after();
+#pragma unroll
+      for (int jb = 0; jb < 2; ++jb) {
+        const int j = 2 * (warp >> 2) + jb;
+        const int cc = 4 * j + q;
+        uint32_t rr[32], rc[32];
+        const uint32_t tb_ = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(j * 96);
+        tmem_ld32(tb_, rr);
+        tmem_ld32(tb_ + 32u, rc);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 32; ++i) rr[i] = __float_as_uint(__uint_as_float(rr[i]) + __uint_as_float(rc[i]));
+        tmem_ld32(tb_ + 64u, rc);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 32; ++i) rr[i] = __float_as_uint(__uint_as_float(rr[i]) + __uint_as_float(rc[i]));
+        const float f = g.out_scale / s_scaleB[cc];
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2)
+          sts64(tb + tile_off<STRIDED>(lane + 32 * k2, cc), __uint_as_float(rr[k2]) * f,
+                __uint_as_float(rr[16 + k2]) * f);
+      }
+      tc_fence_before();
+      fence_proxy_async_smem();  // the tile is next read by the store
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&outrdy[b]);
+    }
+  } else if (warp == 8) {
+    // ---------------- producer ----------------
+    if (lane == 0) {
+      int loads[2] = {0, 0};
+      bool failed = false;
+      auto issue_load = [&](int b, long long tile) {
+        void* dst = sm + (size_t)b * kMixTile;
+        if constexpr (STRIDED) {
+          const int ti = (int)(tile % g.tiles_i);
+          const int o = (int)(tile / g.tiles_i);
+          mbar_expect_tx(&full[b], (uint32_t)kMixTile);
+          for (int kb = 0; kb < g.nlb; ++kb)
+            tma_load_3d(static_cast<unsigned char*>(dst) + (size_t)kb * g.lb * 128, &tin, &full[b], ti * 16,
+                        kb * g.lb, o);
+        } else {
+          const long long q0 = tile * 16;
+          const long long nv = (g.ncols - q0) < 16 ? (g.ncols - q0) : 16;
+          const uint32_t bytes = (uint32_t)(nv * 4096);
+          mbar_expect_tx(&full[b], bytes);
+          bulk_load_1d(dst, static_cast<const unsigned char*>(in) + q0 * 4096, bytes, &full[b]);
+        }
+        ++loads[b];
+      };
+      auto issue_store = [&](int b, long long tile) {
+        const void* src = sm + (size_t)b * kMixTile;
+        if constexpr (STRIDED) {
+          const int ti = (int)(tile % g.tiles_i);
+          const int o = (int)(tile / g.tiles_i);
+          for (int kb = 0; kb < g.nlb; ++kb)
+            tma_store_3d(&tout, static_cast<const unsigned char*>(src) + (size_t)kb * g.lb * 128, ti * 16,
+                         kb * g.lb, o);
+        } else {
+          const long long q0 = tile * 16;
+          const long long nv = (g.ncols - q0) < 16 ? (g.ncols - q0) : 16;
+          bulk_store_1d(static_cast<unsigned char*>(out) + q0 * 4096, src, (uint32_t)(nv * 4096));
+        }
+        bulk_commit();
+      };
+      int it = 0;
+      long long tile = first;
+      // prime both buffers
+      for (; it < 2 && tile < g.ntiles; ++it, tile += step) issue_load(it, tile);
+      // then: store tile it-2 once transformed, refill its buffer with tile it
+      long long done_tile = first;
+      int dit = 0;
+      for (; done_tile < g.ntiles; done_tile += step, ++dit) {
+        const int b = dit & 1;
+        if (!mix_wait(&outrdy[b], (uint32_t)((dit >> 1) & 1), s_abort)) { failed = true; break; }
+        issue_store(b, done_tile);
+        if (tile < g.ntiles) {
+          bulk_wait_read_all();  // the store has read the buffer
+          issue_load(b, tile);
+          tile += step;
+          ++it;
+        }
+      }
+      bulk_wait_all();
+      if (failed) {
+        *s_abort = 1;
+        // loads still in flight land in shared memory: wait for them
+        for (int b = 0; b < 2; ++b)
+          if (loads[b] > 0) mbar_wait_bounded(&full[b], (uint32_t)((loads[b] - 1) & 1));
+      }
+    }
+  } else {
+    // ---------------- MMA issuer (warp 9, lane 0) ----------------
+    if (lane == 0) {
+      const uint32_t opHi = sb + kMixOpA, opLo = opHi + kMixOpBytes;
+      const uint32_t b32h = sb + kMixB32, b32l = b32h + 8192;
+      const uint32_t b16h = sb + kMixB16, b16l = b16h + 4096;
+      constexpr uint32_t idA = umma_idesc_f16(128, 64, 0, 0);
+      constexpr uint32_t idB = umma_idesc_f16(128, 32, 1, 0);
+      int it = 0;
+      uint64_t* last_bar = nullptr;  // the barrier of the last commit, and its phase parity
+      uint32_t last_par = 0;
+      for (long long tile = first; tile < g.ntiles; tile += step, ++it) {
+        if (!mix_wait(opA, (uint32_t)(it & 1), s_abort)) { *s_abort = 1; break; }
+        tc_fence_after();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint32_t d = tmem + (uint32_t)(h * 192);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            const uint32_t ao = (uint32_t)(h * 16384 + s * 32);
+            const uint64_t ah = umma_desc_sw128(opHi + ao, 16, 1024), al = umma_desc_sw128(opLo + ao, 16, 1024);
+            const uint64_t bh = umma_desc_sw128(b32h + s * 32, 16, 1024), bl = umma_desc_sw128(b32l + s * 32, 16, 1024);
+            umma_f16(d + (uint32_t)((s >> 1) * 64), ah, bh, idA, s & 1);  // hi x hi, chains of two
+            umma_f16(d + 128u, al, bh, idA, s > 0);                        // cross terms
+            umma_f16(d + 128u, ah, bl, idA, 1);
+          }
+        }
+        umma_commit(accA);
+        last_bar = accA;
+        last_par = (uint32_t)(it & 1);
+        if (!mix_wait(opB, (uint32_t)(it & 1), s_abort)) { *s_abort = 1; break; }
+        tc_fence_after();
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const uint32_t d = tmem + (uint32_t)(j * 96);
+#pragma unroll
+          for (int s = 0; s < 2; ++s) {
+            const uint32_t ao = (uint32_t)(j * 8192 + s * 2048);
+            const uint64_t ah = umma_desc_sw128(opHi + ao, 4096, 1024), al = umma_desc_sw128(opLo + ao, 4096, 1024);
+            const uint64_t bh = umma_desc_sw128(b16h + s * 32, 16, 1024), bl = umma_desc_sw128(b16l + s * 32, 16, 1024);
+            umma_f16(d + (uint32_t)(32 * s), ah, bh, idB, 0);  // hi x hi, one K-step each
+            umma_f16(d + 64u, al, bh, idB, s > 0);             // cross terms
+            umma_f16(d + 64u, ah, bl, idB, 1);
+          }
+        }
+        umma_commit(accB);
+        last_bar = accB;
+        last_par = (uint32_t)(it & 1);
+      }
+      // products still running read shared memory and write tensor memory:
+      // wait (bounded) for the last commit before the CTA frees either
+      if (last_bar) mbar_wait_bounded(last_bar, last_par);
+    }
+  }
+  if (*s_abort && tid == 0 && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 9) {
+    __syncwarp();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kMixTmemCols)
+                 : "memory");
+  }
+}
+
+}  // namespace dfft

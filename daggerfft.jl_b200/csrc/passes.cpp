@@ -213,6 +213,21 @@ static cudaError_t encode_map(CUtensorMap* m, void* base, const Pass& p) {
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+// Tensor map over {I, L, O} ComplexF32 (8-byte elements) with boxes of 16
+// columns x 256 rows in the 128-byte swizzle the mixed pass reads and writes.
+static cudaError_t encode_map_sw128(CUtensorMap* m, void* base, const Pass& p) {
+  std::call_once(g_encode_once, load_encode);
+  if (!g_encode) return cudaErrorNotSupported;
+  cuuint64_t dims[3] = {(cuuint64_t)p.tI, (cuuint64_t)p.tL, (cuuint64_t)p.tO};
+  cuuint64_t strides[2] = {(cuuint64_t)p.tI * 8, (cuuint64_t)p.tI * 8 * (cuuint64_t)p.tL};
+  cuuint32_t box[3] = {16, (cuuint32_t)p.mgeom.lb, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 static int sm_count() {
   static int v = 0;
   if (!v) {
@@ -967,6 +982,24 @@ cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream,
   PassDesc d = p.d;
   d.in.p = in;
   d.out.p = out;
+  if (p.mixed) {
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
+      return cudaErrorMisalignedAddress;
+    CUtensorMap tin, tout;
+    std::memset(&tin, 0, sizeof(tin));
+    std::memset(&tout, 0, sizeof(tout));
+    if (p.mstrided) {
+      e = encode_map_sw128(&tin, in, p);
+      if (e != cudaSuccess) return e;
+      e = encode_map_sw128(&tout, out, p);
+      if (e != cudaSuccess) return e;
+    }
+    MixedGeom g = p.mgeom;
+    const void* ip = in;
+    void* op = out;
+    void* args[] = {&ip, &op, &tin, &tout, &g};
+    return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
+  }
   if (p.tiled) {
     if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
       return cudaErrorMisalignedAddress;

@@ -79,8 +79,11 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
   for (int a : ax)
     if (S[a] > 0x7fffffffLL) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "axis too long"};
 
-  if (method == DFFT_MIXED)
-    throw Error{DFFT_ERROR_INVALID_VALUE, "the mixed tensor-core form is not built in this version"};
+  // the mixed (tensor-core) form covers complex transforms; its passes run
+  // the ComplexF32 axes of length 512, the other axes (and ComplexF64) keep
+  // the plain form
+  if (method == DFFT_MIXED && !is_c2c(transform))
+    throw Error{DFFT_ERROR_INVALID_VALUE, "the mixed form covers complex (FFT / IFFT) transforms"};
 
   size_t chirp_bytes = 0;
   auto add = [&](const PassSpec& sp, int src, int dst) {
@@ -129,6 +132,19 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
     };
     for (size_t i = 0; i < order.size(); ++i) {
       const int a = order[i];
+      if (method == DFFT_MIXED) {
+        PassSpec s = axis_spec(a);
+        if (mixed_supported(dbl, s.L, s.I)) {
+          Pass m = make_mixed_pass(s.I, s.O, inv ? 1 : 0);
+          m.src = src;
+          m.dst = BUF_OUT;
+          P->passes.push_back(std::move(m));
+        } else {
+          add(s, src, BUF_OUT);
+        }
+        src = BUF_OUT;
+        continue;
+      }
       // dims 1 and 2 adjacent in the stage order of an L x L x O array: one
       // fused 2-D pass per slab (src/fft.jl:735 transforms each slab along
       // dims (1, 2) before the exchange) when it beats the per-axis passes
