@@ -30,21 +30,26 @@
 // exact.
 //
 // Tile: 16 pencils (columns of a strided axis, or whole contiguous pencils)
-// x 512 points, 64 KB of ComplexF32.  Stage A is M = 256 rows (pencil c,
-// n2) x N = 64 x K = 64, two M = 128 MMAs per K-step; stage B is M = 512
-// rows (c, k1) x N = 32 x K = 32, four M = 128 MMAs per K-step.  TMEM (512
-// columns): stage A block h at 192 h (hi x hi K-steps 0-1 at +0, 2-3 at +64,
-// cross terms at +128); stage B block j at 96 j (hi x hi K-step 0 at +0,
-// K-step 1 at +32, cross terms at +64), reusing stage A's columns once its
-// epilogue has read them.
+// x 512 points, 64 KB of ComplexF32, worked on by two groups of 8 pencils.
+// Per group, stage A is M = 128 rows (pencil, n2) x N = 64 x K = 64, one
+// M = 128 MMA per K-step; stage B is M = 256 rows (pencil, k1) x N = 32 x
+// K = 32, two M = 128 MMAs per K-step.  TMEM (512 columns, 256 per group):
+// stage A at +0 (hi x hi K-steps 0-1), +64 (K-steps 2-3), +128 (cross
+// terms); stage B block j at 96 j (hi x hi K-step 0 at +0, K-step 1 at +32,
+// cross terms at +64), reusing stage A's columns once its epilogue has read
+// them.
 //
 // Warp roles (320 threads, one CTA per SM, persistent over tiles):
-//   warps 0-7  convert / epilogue threads: thread t owns stage-A row t =
-//              (c = t/16, n2 = t%16) -- its prep (FP32 tile -> scaled FP16
-//              hi/lo, K-major 128B-swizzled rows), its TMEM row in the stage-A
-//              epilogue (unscale, twiddle, rescale, split into the stage-B
-//              operand, MN-major 128B-swizzled) -- and two stage-B rows
-//              (c, k1) in the final epilogue (unscale, store FP32).
+//   warps 0-7  convert / epilogue threads in two independent groups of four
+//              warps, group gr owning pencils 8gr..8gr+7 of every tile with
+//              its own operand buffer (32 KB), 256 TMEM columns and
+//              barriers, so that one group's conversions overlap the other
+//              group's products.  Thread tl of a group owns stage-A row tl =
+//              (pencil tl/16, n2 = tl%16) -- its prep (FP32 tile -> scaled
+//              FP16 hi/lo, K-major 128B-swizzled rows), its TMEM row in the
+//              stage-A epilogue (unscale, twiddle, rescale, split into the
+//              stage-B operand, MN-major 128B-swizzled) -- and two stage-B
+//              rows (pencil, k1) in the final epilogue (unscale, store FP32).
 //   warp 8     producer: TMA / bulk loads into two tile buffers, TMA / bulk
 //              stores of finished tiles.
 //   warp 9     TMEM allocation; lane 0 issues the tcgen05.mma products and
@@ -136,18 +141,32 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t* r) {
 #undef DFFT_R8
 
 // Power-of-two scale that puts a pencil maximum m in [2^14, 2^15) (clamped
-// to the normal range; m = 0 gives a harmless large scale).
+// so that the scale and its reciprocal are normal; m = 0 gives a harmless
+// large scale).
 __device__ __forceinline__ float mix_scale(float m) {
   int e = (int)((__float_as_uint(m) >> 23) & 0xFF);
   int b = 268 - e;
-  b = b < 1 ? 1 : (b > 254 ? 254 : b);
+  b = b < 1 ? 1 : (b > 253 ? 253 : b);
   return __uint_as_float((uint32_t)b << 23);
+}
+// The reciprocal of a scale from mix_scale (exact: a power of two).
+__device__ __forceinline__ float mix_inv(float s) {
+  return __uint_as_float((254u - (__float_as_uint(s) >> 23)) << 23);
+}
+// x rounded to 11 significant bits (ties away from zero) with integer
+// operations: the result is exactly representable in FP16 in its normal
+// range, so its FP16 conversion is exact and the residual x - r11(x) is
+// exact in FP32.  (Converting the FP16 hi part back to FP32 instead would
+// run two more conversions per pair on the quarter-rate conversion pipe,
+// which the FP16 packs already load.)
+__device__ __forceinline__ float r11(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 // FP16 hi / lo split of a pair of FP32 values (already scaled).
 __device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
-  const __half2 h = __floats2half2_rn(a, b);
-  const float2 f = __half22float2(h);
-  const __half2 l = __floats2half2_rn(a - f.x, b - f.y);
+  const float ha = r11(a), hb = r11(b);
+  const __half2 h = __floats2half2_rn(ha, hb);
+  const __half2 l = __floats2half2_rn(a - ha, b - hb);
   hi = *reinterpret_cast<const uint32_t*>(&h);
   lo = *reinterpret_cast<const uint32_t*>(&l);
 }
@@ -194,8 +213,8 @@ template <bool STRIDED> __device__ __forceinline__ uint32_t tile_off(int k, int 
 
 // STRIDED: the axis has element stride I > 1 (tile = 16 adjacent columns,
 // TMA boxes {16, lb, 1} of the tensor {I, 512, O}); otherwise the axis is
-// contiguous (tile = 16 whole pencils, one bulk copy).  DIR: 1 forward, 2
-// inverse (selects the DFT matrices and twiddles in `consts`).
+// contiguous (tile = 16 whole pencils, one bulk copy).  The direction is in
+// `consts` (DFT matrices and twiddles) and g.out_scale.
 template <bool STRIDED>
 __global__ void __launch_bounds__(kMixThreads, 1)
     mixed_pass(const void* in, void* out, const __grid_constant__ CUtensorMap tin,
@@ -207,23 +226,24 @@ __global__ void __launch_bounds__(kMixThreads, 1)
   const uint32_t sb = raw + pad;  // aligned base (shared address)
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kMixMisc);
   uint64_t* full = bars;        // [2] tile loaded
-  uint64_t* outrdy = bars + 2;  // [2] tile transformed
-  uint64_t* opA = bars + 4;     // stage-A operands written
-  uint64_t* opB = bars + 5;     // stage-B operands written
-  uint64_t* accA = bars + 6;    // stage-A products done
-  uint64_t* accB = bars + 7;    // stage-B products done
-  uint64_t* scl = bars + 8;     // stage-B pencil scales written
-  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + kMixMisc + 96);
-  volatile int* s_abort = reinterpret_cast<volatile int*>(sm + kMixMisc + 100);
+  uint64_t* outrdy = bars + 2;  // [2] tile transformed (both groups)
+  uint64_t* opA = bars + 4;     // [2] per group: stage-A operands written
+  uint64_t* opB = bars + 6;     // [2] stage-B operands written
+  uint64_t* accA = bars + 8;    // [2] stage-A products done
+  uint64_t* accB = bars + 10;   // [2] stage-B products done
+  uint64_t* scl = bars + 12;    // [2] stage-B pencil scales written
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + kMixMisc + 112);
+  volatile int* s_abort = reinterpret_cast<volatile int*>(sm + kMixMisc + 116);
   float* s_scaleB = reinterpret_cast<float*>(sm + kMixMisc + 128);  // [16]
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   volatile int* verr = g.err;
 
   if (tid == 0) {
-    // full, accA, accB: one arrival (expect_tx / tcgen05.commit); outrdy,
-    // opA, opB, scl: one arrival per convert warp
-    for (int i = 0; i < 9; ++i) mbar_init(&bars[i], (i == 0 || i == 1 || i == 6 || i == 7) ? 1 : 8);
+    // full, accA, accB: one arrival (expect_tx / tcgen05.commit); outrdy:
+    // one per convert warp; opA, opB, scl: one per warp of the group
+    for (int i = 0; i < 14; ++i)
+      mbar_init(&bars[i], (i < 2 || (i >= 8 && i < 12)) ? 1 : (i < 4 ? 8 : 4));
     mbar_fence_init();
     *s_abort = 0;
   }
@@ -249,16 +269,22 @@ __global__ void __launch_bounds__(kMixThreads, 1)
 
   if (warp < 8) {
     // ---------------- convert / epilogue threads ----------------
-    const int c = tid >> 4, n2 = tid & 15;
-    const int q = warp & 3;
-    const uint32_t opHi = sb + kMixOpA, opLo = opHi + kMixOpBytes;
+    // group gr = warps 4gr..4gr+3: pencils 8gr..8gr+7 of every tile, its own
+    // operand buffer, tensor memory (256 columns) and barriers
+    const int gr = warp >> 2, q = warp & 3;
+    const int tl = tid & 127;                  // stage-A row of the group
+    const int cl = tl >> 4, n2 = tl & 15;      // pencil within the group, n2
+    const int c = 8 * gr + cl;                 // pencil within the tile
+    const uint32_t opHi = sb + kMixOpA + (uint32_t)gr * 32768u, opLo = opHi + 16384u;
     const uint32_t twb = sb + kMixTw;
+    const uint32_t tg = tmem + (uint32_t)gr * 256u + ((uint32_t)(q * 32) << 16);
     int it = 0;
     for (long long tile = first; tile < g.ntiles; tile += step, ++it) {
       const int b = it & 1;
+      const uint32_t par = (uint32_t)(it & 1);
       if (!mix_wait_warp(&full[b], (uint32_t)((it >> 1) & 1), s_abort)) { *s_abort = 1; break; }
       const uint32_t tb = sb + (uint32_t)b * kMixTile;
-      // ---- stage-A operands: row t = (c, n2), K = [re n1 0..31 | im n1 0..31]
+      // ---- stage-A operands: row tl = (cl, n2), K = [re n1 0..31 | im n1 0..31]
       float2 v[32];
 #pragma unroll
       for (int n1 = 0; n1 < 32; ++n1) v[n1] = lds64(tb + tile_off<STRIDED>(16 * n1 + n2, c));
@@ -269,8 +295,8 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       for (int o = 8; o >= 1; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
       const float sA = mix_scale(m);
       {
-        const uint32_t row = (uint32_t)tid * 128u;
-        const int r8 = tid & 7;
+        const uint32_t row = (uint32_t)tl * 128u;
+        const int r8 = tl & 7;
 #pragma unroll
         for (int jj = 0; jj < 8; ++jj) {
           uint32_t h[4], l[4];
@@ -288,28 +314,25 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       }
       fence_proxy_async_smem();
       __syncwarp();
-      if (lane == 0) mbar_arrive(opA);
-      // ---- stage-A epilogue: TMEM row t -> unscale, twiddle, rescale, split
-      if (!mix_wait_warp(accA, (uint32_t)(it & 1), s_abort)) { *s_abort = 1; break; }
+      if (lane == 0) mbar_arrive(&opA[gr]);
+      // ---- stage-A epilogue: TMEM row tl -> unscale, twiddle, rescale, split
+      if (!mix_wait_warp(&accA[gr], par, s_abort)) { *s_abort = 1; break; }
       tc_fence_after();
       uint32_t r[64];
-      {
-        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((warp >> 2) * 192);
 #pragma unroll
-        for (int part = 0; part < 2; ++part) {  // real parts (columns 0-31), then imaginary
-          uint32_t t0[32], t1[32];
-          tmem_ld32(ta + (uint32_t)(32 * part), t0);
-          tmem_ld32(ta + 64u + (uint32_t)(32 * part), t1);
-          tmem_wait_ld();
+      for (int part = 0; part < 2; ++part) {  // real parts (columns 0-31), then imaginary
+        uint32_t t0[32], t1[32];
+        tmem_ld32(tg + (uint32_t)(32 * part), t0);
+        tmem_ld32(tg + 64u + (uint32_t)(32 * part), t1);
+        tmem_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 32; ++i) r[32 * part + i] = __float_as_uint(__uint_as_float(t0[i]) + __uint_as_float(t1[i]));
-          tmem_ld32(ta + 128u + (uint32_t)(32 * part), t0);
-          tmem_wait_ld();
+        for (int i = 0; i < 32; ++i) r[32 * part + i] = __float_as_uint(__uint_as_float(t0[i]) + __uint_as_float(t1[i]));
+        tmem_ld32(tg + 128u + (uint32_t)(32 * part), t0);
+        tmem_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 32; ++i) r[32 * part + i] = __float_as_uint(__uint_as_float(r[32 * part + i]) + __uint_as_float(t0[i]));
-        }
+        for (int i = 0; i < 32; ++i) r[32 * part + i] = __float_as_uint(__uint_as_float(r[32 * part + i]) + __uint_as_float(t0[i]));
       }
-      const float iA = 1.0f / sA;  // exact: a power of two
+      const float iA = mix_inv(sA);
       float mb = 0.f;
 #pragma unroll
       for (int k1 = 0; k1 < 32; ++k1) {
@@ -325,15 +348,15 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       const float sB = mix_scale(mb);
       if (n2 == 0) s_scaleB[c] = sB;
       __syncwarp();
-      if (lane == 0) mbar_arrive(scl);
+      if (lane == 0) mbar_arrive(&scl[gr]);
       tc_fence_before();
       {
-        // stage-B operand, MN-major: M = c*32 + k1 (atoms of 64 rows, 4 KB
+        // stage-B operand, MN-major: M = cl*32 + k1 (atoms of 64 rows, 4 KB
         // apart), K = [re n2 0..15 | im n2 0..15] (groups of 8 rows, 1 KB apart)
         const int kr = n2 & 7;
 #pragma unroll
         for (int part = 0; part < 2; ++part) {
-          const uint32_t kbase = (uint32_t)((c >> 1) * 4096 + (2 * part + (n2 >> 3)) * 1024 + kr * 128);
+          const uint32_t kbase = (uint32_t)((cl >> 1) * 4096 + (2 * part + (n2 >> 3)) * 1024 + kr * 128);
 #pragma unroll
           for (int jj = 0; jj < 4; ++jj) {
             uint32_t h[4], l[4];
@@ -343,7 +366,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
               split2(__uint_as_float(r[32 * part + k1]) * sB, __uint_as_float(r[32 * part + k1 + 1]) * sB, h[e],
                      l[e]);
             }
-            const uint32_t off = kbase + (uint32_t)(((((c & 1) * 4 + jj) ^ kr) << 4));
+            const uint32_t off = kbase + (uint32_t)(((((cl & 1) * 4 + jj) ^ kr) << 4));
             sts128(opHi + off, h[0], h[1], h[2], h[3]);
             sts128(opLo + off, l[0], l[1], l[2], l[3]);
           }
@@ -351,19 +374,18 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       }
       fence_proxy_async_smem();
       __syncwarp();
-      if (lane == 0) mbar_arrive(opB);
-      // ---- stage-B epilogue: rows (c' = 4j + q, k1 = lane), j = 2*(warp/4) + jb
-      if (!mix_wait_warp(accB, (uint32_t)(it & 1), s_abort) || !mix_wait_warp(scl, (uint32_t)(it & 1), s_abort)) {
+      if (lane == 0) mbar_arrive(&opB[gr]);
+      // ---- stage-B epilogue: rows (cl = 4j + q, k1 = lane) of blocks j = 0, 1
+      if (!mix_wait_warp(&accB[gr], par, s_abort) || !mix_wait_warp(&scl[gr], par, s_abort)) {
         *s_abort = 1;
         break;
       }
       tc_fence_after();
 #pragma unroll
-      for (int jb = 0; jb < 2; ++jb) {
-        const int j = 2 * (warp >> 2) + jb;
-        const int cc = 4 * j + q;
+      for (int j = 0; j < 2; ++j) {
+        const int cc = 8 * gr + 4 * j + q;
         uint32_t rr[32], rc[32];
-        const uint32_t tb_ = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(j * 96);
+        const uint32_t tb_ = tg + (uint32_t)(j * 96);
         tmem_ld32(tb_, rr);
         tmem_ld32(tb_ + 32u, rc);
         tmem_wait_ld();
@@ -373,7 +395,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         tmem_wait_ld();
 #pragma unroll
         for (int i = 0; i < 32; ++i) rr[i] = __float_as_uint(__uint_as_float(rr[i]) + __uint_as_float(rc[i]));
-        const float f = g.out_scale / s_scaleB[cc];
+        const float f = g.out_scale * mix_inv(s_scaleB[cc]);
 #pragma unroll
         for (int k2 = 0; k2 < 16; ++k2)
           sts64(tb + tile_off<STRIDED>(lane + 32 * k2, cc), __uint_as_float(rr[k2]) * f,
@@ -426,7 +448,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       long long tile = first;
       // prime both buffers
       for (; it < 2 && tile < g.ntiles; ++it, tile += step) issue_load(it, tile);
-      // then: store tile it-2 once transformed, refill its buffer with tile it
+      // then: store tile dit once transformed, refill its buffer with the next tile
       long long done_tile = first;
       int dit = 0;
       for (; done_tile < g.ntiles; done_tile += step, ++dit) {
@@ -450,56 +472,84 @@ __global__ void __launch_bounds__(kMixThreads, 1)
     }
   } else {
     // ---------------- MMA issuer (warp 9, lane 0) ----------------
+    // serves the two groups in the order their operands become ready
     if (lane == 0) {
-      const uint32_t opHi = sb + kMixOpA, opLo = opHi + kMixOpBytes;
       const uint32_t b32h = sb + kMixB32, b32l = b32h + 8192;
       const uint32_t b16h = sb + kMixB16, b16l = b16h + 4096;
       constexpr uint32_t idA = umma_idesc_f16(128, 64, 0, 0);
       constexpr uint32_t idB = umma_idesc_f16(128, 32, 1, 0);
-      int it = 0;
-      uint64_t* last_bar = nullptr;  // the barrier of the last commit, and its phase parity
-      uint32_t last_par = 0;
-      for (long long tile = first; tile < g.ntiles; tile += step, ++it) {
-        if (!mix_wait(opA, (uint32_t)(it & 1), s_abort)) { *s_abort = 1; break; }
-        tc_fence_after();
+      const long long ntile = g.ntiles > first ? (g.ntiles - first + step - 1) / step : 0;
+      long long done[2] = {0, 0};  // tiles each group has had both stages issued for
+      int stage[2] = {0, 0};       // next request: 0 stage A, 1 stage B
+      uint64_t* last_bar[2] = {nullptr, nullptr};  // last commit per group, and its phase parity
+      uint32_t last_par[2] = {0, 0};
+      const uint64_t t0 = global_ns();
+      uint64_t t_last = t0;
+      unsigned spins = 0;
+      while ((done[0] < ntile || done[1] < ntile) && !*s_abort) {
+        bool progressed = false;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const uint32_t d = tmem + (uint32_t)(h * 192);
+        for (int gq = 0; gq < 2; ++gq) {
+          if (done[gq] >= ntile) continue;
+          const uint32_t par = (uint32_t)(done[gq] & 1);
+          const uint32_t opHi = sb + kMixOpA + (uint32_t)gq * 32768u, opLo = opHi + 16384u;
+          const uint32_t d = tmem + (uint32_t)gq * 256u;
+          if (stage[gq] == 0) {
+            if (!mbar_try_wait(&opA[gq], par)) continue;
+            tc_fence_after();
 #pragma unroll
-          for (int s = 0; s < 4; ++s) {
-            const uint32_t ao = (uint32_t)(h * 16384 + s * 32);
-            const uint64_t ah = umma_desc_sw128(opHi + ao, 16, 1024), al = umma_desc_sw128(opLo + ao, 16, 1024);
-            const uint64_t bh = umma_desc_sw128(b32h + s * 32, 16, 1024), bl = umma_desc_sw128(b32l + s * 32, 16, 1024);
-            umma_f16(d + (uint32_t)((s >> 1) * 64), ah, bh, idA, s & 1);  // hi x hi, chains of two
-            umma_f16(d + 128u, al, bh, idA, s > 0);                        // cross terms
-            umma_f16(d + 128u, ah, bl, idA, 1);
+            for (int s = 0; s < 4; ++s) {
+              const uint32_t ao = (uint32_t)(s * 32);
+              const uint64_t ah = umma_desc_sw128(opHi + ao, 16, 1024), al = umma_desc_sw128(opLo + ao, 16, 1024);
+              const uint64_t bh = umma_desc_sw128(b32h + s * 32, 16, 1024), bl = umma_desc_sw128(b32l + s * 32, 16, 1024);
+              umma_f16(d + (uint32_t)((s >> 1) * 64), ah, bh, idA, s & 1);  // hi x hi, chains of two
+              umma_f16(d + 128u, al, bh, idA, s > 0);                        // cross terms
+              umma_f16(d + 128u, ah, bl, idA, 1);
+            }
+            umma_commit(&accA[gq]);
+            last_bar[gq] = &accA[gq];
+            last_par[gq] = par;
+            stage[gq] = 1;
+          } else {
+            if (!mbar_try_wait(&opB[gq], par)) continue;
+            tc_fence_after();
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+              const uint32_t dj = d + (uint32_t)(j * 96);
+#pragma unroll
+              for (int s = 0; s < 2; ++s) {
+                const uint32_t ao = (uint32_t)(j * 8192 + s * 2048);
+                const uint64_t ah = umma_desc_sw128(opHi + ao, 4096, 1024), al = umma_desc_sw128(opLo + ao, 4096, 1024);
+                const uint64_t bh = umma_desc_sw128(b16h + s * 32, 16, 1024), bl = umma_desc_sw128(b16l + s * 32, 16, 1024);
+                umma_f16(dj + (uint32_t)(32 * s), ah, bh, idB, 0);  // hi x hi, one K-step each
+                umma_f16(dj + 64u, al, bh, idB, s > 0);             // cross terms
+                umma_f16(dj + 64u, ah, bl, idB, 1);
+              }
+            }
+            umma_commit(&accB[gq]);
+            last_bar[gq] = &accB[gq];
+            last_par[gq] = par;
+            stage[gq] = 0;
+            ++done[gq];
           }
+          progressed = true;
         }
-        umma_commit(accA);
-        last_bar = accA;
-        last_par = (uint32_t)(it & 1);
-        if (!mix_wait(opB, (uint32_t)(it & 1), s_abort)) { *s_abort = 1; break; }
-        tc_fence_after();
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const uint32_t d = tmem + (uint32_t)(j * 96);
-#pragma unroll
-          for (int s = 0; s < 2; ++s) {
-            const uint32_t ao = (uint32_t)(j * 8192 + s * 2048);
-            const uint64_t ah = umma_desc_sw128(opHi + ao, 4096, 1024), al = umma_desc_sw128(opLo + ao, 4096, 1024);
-            const uint64_t bh = umma_desc_sw128(b16h + s * 32, 16, 1024), bl = umma_desc_sw128(b16l + s * 32, 16, 1024);
-            umma_f16(d + (uint32_t)(32 * s), ah, bh, idB, 0);  // hi x hi, one K-step each
-            umma_f16(d + 64u, al, bh, idB, s > 0);             // cross terms
-            umma_f16(d + 64u, ah, bl, idB, 1);
-          }
+        if (progressed) {
+          t_last = global_ns();
+          spins = 0;
+        } else if ((++spins & 255) == 0 && global_ns() - t_last > kWaitNs) {
+          *s_abort = 1;  // neither group handed over operands in time
+          break;
+        } else if (spins > kWaitLimit) {
+          *s_abort = 1;
+          break;
         }
-        umma_commit(accB);
-        last_bar = accB;
-        last_par = (uint32_t)(it & 1);
       }
+      (void)t0;
       // products still running read shared memory and write tensor memory:
-      // wait (bounded) for the last commit before the CTA frees either
-      if (last_bar) mbar_wait_bounded(last_bar, last_par);
+      // wait (bounded) for each group's last commit before the CTA frees either
+      for (int gq = 0; gq < 2; ++gq)
+        if (last_bar[gq]) mbar_wait_bounded(last_bar[gq], last_par[gq]);
     }
   }
   if (*s_abort && tid == 0 && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
