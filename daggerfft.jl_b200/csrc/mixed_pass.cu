@@ -95,8 +95,9 @@ std::shared_ptr<DevTable> mixed_consts(int inverse) {
   for (int n2 = 0; n2 < 16; ++n2)
     for (int k1 = 0; k1 < 32; ++k1) {
       const long double ang = 2 * kPi * (long double)((n2 * k1) % 512) / 512.0L;
-      tw[2 * (n2 * 33 + k1)] = (float)cosl(ang);
-      tw[2 * (n2 * 33 + k1) + 1] = (float)(sign * sinl(ang));
+      // W512^(n2 k1) / 32: the stage-B operands carry the stage-A scale / 32
+      tw[2 * (n2 * 33 + k1)] = (float)(cosl(ang) / 32);
+      tw[2 * (n2 * 33 + k1) + 1] = (float)(sign * sinl(ang) / 32);
     }
   auto t = std::make_shared<DevTable>();
   t->device = dev;

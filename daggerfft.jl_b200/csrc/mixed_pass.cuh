@@ -13,7 +13,12 @@
 // shared memory, FP64-generated).  Operands are FP16 hi + lo splits of FP32
 // values: D = A_hi B_hi + A_lo B_hi + A_hi B_lo, accumulated in FP32 in
 // tensor memory (the dropped A_lo B_lo term and the split residuals are
-// about 2^-22 of each value).  The tensor cores round each MMA's FP32
+// about 2^-22 of each value).  Per-pencil scaling: stage A's operands are
+// scaled by a power of two sA that puts the pencil's largest |re|, |im| in
+// [2^14, 2^15); stage B's by sA / 32 (|Y| <= 32 max|x|, so the bound holds
+// without a second reduction, and the 1/32 rides on the twiddle table);
+// the epilogue multiplies by 32 / sA (and 1/512 for the inverse), all exact
+// powers of two.  The tensor cores round each MMA's FP32
 // accumulation toward zero, so a long chain of K-steps into one accumulator
 // shrinks every result by a few ulps (a bias that adds up over passes: a
 // 12-step chain measured 1.75e-6 over a 4-pass round trip).  The products
@@ -28,6 +33,10 @@
 // precision follow each pencil's own magnitude); the scale is undone
 // exactly after the product.  Twiddles and the inverse's 1/512 stay FP32 /
 // exact.
+//
+// (Each value's FP16 hi + lo split keeps about 22 bits relative to the value
+// itself, so a scale set by a bound rather than the exact maximum only
+// matters for values far below the pencil's norm.)
 //
 // Tile: 16 pencils (columns of a strided axis, or whole contiguous pencils)
 // x 512 points, 64 KB of ComplexF32, worked on by two groups of 8 pencils.
@@ -108,6 +117,15 @@ __device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b
       "l"(a), "l"(b), "r"(idesc), "r"(acc)
       : "memory");
 }
+// The same with the A operand in tensor memory (row m in lane m, K packed
+// two FP16 values per 32-bit column).
+__device__ __forceinline__ void umma_f16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc, int acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    smem_u32(bar))
@@ -120,6 +138,7 @@ __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 #define DFFT_R8(i) "=r"(r[i]), "=r"(r[i + 1]), "=r"(r[i + 2]), "=r"(r[i + 3]), "=r"(r[i + 4]), \
                    "=r"(r[i + 5]), "=r"(r[i + 6]), "=r"(r[i + 7])
@@ -138,6 +157,16 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t* r) {
       : DFFT_R8(0), DFFT_R8(8), DFFT_R8(16), DFFT_R8(24), DFFT_R8(32), DFFT_R8(40), DFFT_R8(48), DFFT_R8(56)
       : "r"(taddr));
 }
+#define DFFT_W8(i) "r"(r[i]), "r"(r[i + 1]), "r"(r[i + 2]), "r"(r[i + 3]), "r"(r[i + 4]), \
+                   "r"(r[i + 5]), "r"(r[i + 6]), "r"(r[i + 7])
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t* r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+      DFFT_W8(0), DFFT_W8(8), DFFT_W8(16), DFFT_W8(24)
+      : "memory");
+}
+#undef DFFT_W8
 #undef DFFT_R8
 
 // Power-of-two scale that puts a pencil maximum m in [2^14, 2^15) (clamped
@@ -187,6 +216,7 @@ __device__ __forceinline__ bool mix_wait(uint64_t* bar, uint32_t parity, volatil
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   for (unsigned i = 1; i < kWaitLimit; ++i) {
+    __nanosleep(32);  // leave the issue slots and the shared-memory pipe to the working warps
     if (mbar_try_wait(bar, parity)) return true;
     if ((i & 255) == 0) {
       if (*abort_flag) return false;
@@ -202,6 +232,13 @@ __device__ __forceinline__ bool mix_wait_warp(uint64_t* bar, uint32_t parity, vo
   const bool ok = mix_wait(bar, parity, abort_flag);
   return __all_sync(0xffffffffu, ok) != 0;
 }
+
+// Stage-B row blocks: M = pos(cl) * 32 + k1 for pencil cl (0..7) of a
+// group: pencils 2q and 2q + 1 land in row blocks 0 and 1 of warp quarter
+// q, the warp whose stage-A rows they were (so their scales are in its
+// lanes), and a strided tile's final epilogue holds both columns of a
+// 16-byte chunk of the 128-byte swizzled tile row.
+__device__ __forceinline__ int mix_pos(int cl) { return 4 * (cl & 1) + (cl >> 1); }
 
 // Byte offset of element (k, c) of a tile: strided tiles are [k][c] rows of
 // 16 complex (128 bytes) in TMA's 128-byte swizzle; contiguous tiles are
@@ -231,21 +268,20 @@ __global__ void __launch_bounds__(kMixThreads, 1)
   uint64_t* opB = bars + 6;     // [2] stage-B operands written
   uint64_t* accA = bars + 8;    // [2] stage-A products done
   uint64_t* accB = bars + 10;   // [2] stage-B products done
-  uint64_t* scl = bars + 12;    // [2] stage-B pencil scales written
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + kMixMisc + 112);
   volatile int* s_abort = reinterpret_cast<volatile int*>(sm + kMixMisc + 116);
-  float* s_scaleB = reinterpret_cast<float*>(sm + kMixMisc + 128);  // [16]
+  volatile int* s_g0 = reinterpret_cast<volatile int*>(sm + kMixMisc + 120);  // group 0's last prepped tile
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   volatile int* verr = g.err;
 
   if (tid == 0) {
     // full, accA, accB: one arrival (expect_tx / tcgen05.commit); outrdy:
-    // one per convert warp; opA, opB, scl: one per warp of the group
-    for (int i = 0; i < 14; ++i)
-      mbar_init(&bars[i], (i < 2 || (i >= 8 && i < 12)) ? 1 : (i < 4 ? 8 : 4));
+    // one per convert warp; opA, opB: one per warp of the group
+    for (int i = 0; i < 12; ++i) mbar_init(&bars[i], (i < 2 || i >= 8) ? 1 : (i < 4 ? 8 : 4));
     mbar_fence_init();
     *s_abort = 0;
+    *s_g0 = -1;
   }
   // constants: DFT operand images and the twiddle table
   {
@@ -283,6 +319,22 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       const int b = it & 1;
       const uint32_t par = (uint32_t)(it & 1);
       if (!mix_wait_warp(&full[b], (uint32_t)((it >> 1) & 1), s_abort)) { *s_abort = 1; break; }
+      // group 1 runs half a step behind group 0 (its prep starts once group
+      // 0's stage-A products are queued), so that each group's conversions
+      // overlap the other group's products instead of competing with them
+      if (gr == 1) {
+        // a monotonic counter, not a barrier phase: group 0 may be more than
+        // one phase ahead
+        bool ok = true;
+        if (*s_g0 < it) {
+          const uint64_t t0 = global_ns();
+          while (*s_g0 < it) {
+            __nanosleep(32);
+            if (*s_abort || global_ns() - t0 > kWaitNs) { ok = false; break; }
+          }
+        }
+        if (!__all_sync(0xffffffffu, ok)) { *s_abort = 1; break; }
+      }
       const uint32_t tb = sb + (uint32_t)b * kMixTile;
       // ---- stage-A operands: row tl = (cl, n2), K = [re n1 0..31 | im n1 0..31]
       float2 v[32];
@@ -295,27 +347,25 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       for (int o = 8; o >= 1; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
       const float sA = mix_scale(m);
       {
-        const uint32_t row = (uint32_t)tl * 128u;
-        const int r8 = tl & 7;
+        // the row goes to tensor memory (lane tl of the group's columns
+        // 192-223 hi, 224-255 lo): word w holds K = 2w, 2w + 1
+        uint32_t hw[32], lw[32];
 #pragma unroll
-        for (int jj = 0; jj < 8; ++jj) {
-          uint32_t h[4], l[4];
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int n1 = 8 * (jj & 3) + 2 * e;
-            const float a0 = (jj < 4 ? v[n1].x : v[n1].y) * sA;
-            const float a1 = (jj < 4 ? v[n1 + 1].x : v[n1 + 1].y) * sA;
-            split2(a0, a1, h[e], l[e]);
-          }
-          const uint32_t off = row + (uint32_t)(((jj ^ r8) << 4));
-          sts128(opHi + off, h[0], h[1], h[2], h[3]);
-          sts128(opLo + off, l[0], l[1], l[2], l[3]);
+        for (int w = 0; w < 32; ++w) {
+          const int n1 = (2 * w) & 31;
+          const float a0 = (w < 16 ? v[n1].x : v[n1].y) * sA;
+          const float a1 = (w < 16 ? v[n1 + 1].x : v[n1 + 1].y) * sA;
+          split2(a0, a1, hw[w], lw[w]);
         }
+        tmem_st32(tg + 192u, hw);
+        tmem_st32(tg + 224u, lw);
+        tmem_wait_st();
       }
-      fence_proxy_async_smem();
+      tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&opA[gr]);
-      // ---- stage-A epilogue: TMEM row tl -> unscale, twiddle, rescale, split
+      if (gr == 0 && q == 0 && lane == 0) *s_g0 = it;
+      // ---- stage-A epilogue: TMEM row tl -> twiddle (and 1/32), split
       if (!mix_wait_warp(&accA[gr], par, s_abort)) { *s_abort = 1; break; }
       tc_fence_after();
       uint32_t r[64];
@@ -332,41 +382,33 @@ __global__ void __launch_bounds__(kMixThreads, 1)
 #pragma unroll
         for (int i = 0; i < 32; ++i) r[32 * part + i] = __float_as_uint(__uint_as_float(r[32 * part + i]) + __uint_as_float(t0[i]));
       }
-      const float iA = mix_inv(sA);
-      float mb = 0.f;
+      // the values carry the stage-A scale sA; the twiddles carry 1/32, so
+      // the stage-B operands come out scaled by sA / 32
 #pragma unroll
       for (int k1 = 0; k1 < 32; ++k1) {
         const float2 w = lds64(twb + (uint32_t)((n2 * 33 + k1) * 8));
-        const float yr = __uint_as_float(r[k1]) * iA, yi = __uint_as_float(r[32 + k1]) * iA;
-        const float zr = yr * w.x - yi * w.y, zi = yr * w.y + yi * w.x;
-        r[k1] = __float_as_uint(zr);
-        r[32 + k1] = __float_as_uint(zi);
-        mb = fmaxf(mb, fmaxf(fabsf(zr), fabsf(zi)));
+        const float yr = __uint_as_float(r[k1]), yi = __uint_as_float(r[32 + k1]);
+        r[k1] = __float_as_uint(yr * w.x - yi * w.y);
+        r[32 + k1] = __float_as_uint(yr * w.y + yi * w.x);
       }
-#pragma unroll
-      for (int o = 8; o >= 1; o >>= 1) mb = fmaxf(mb, __shfl_xor_sync(0xffffffffu, mb, o));
-      const float sB = mix_scale(mb);
-      if (n2 == 0) s_scaleB[c] = sB;
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&scl[gr]);
       tc_fence_before();
       {
-        // stage-B operand, MN-major: M = cl*32 + k1 (atoms of 64 rows, 4 KB
+        // stage-B operand, MN-major: M = pos*32 + k1 (atoms of 64 rows, 4 KB
         // apart), K = [re n2 0..15 | im n2 0..15] (groups of 8 rows, 1 KB apart)
         const int kr = n2 & 7;
+        const int pos = mix_pos(cl);
 #pragma unroll
         for (int part = 0; part < 2; ++part) {
-          const uint32_t kbase = (uint32_t)((cl >> 1) * 4096 + (2 * part + (n2 >> 3)) * 1024 + kr * 128);
+          const uint32_t kbase = (uint32_t)((pos >> 1) * 4096 + (2 * part + (n2 >> 3)) * 1024 + kr * 128);
 #pragma unroll
           for (int jj = 0; jj < 4; ++jj) {
             uint32_t h[4], l[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
               const int k1 = 8 * jj + 2 * e;
-              split2(__uint_as_float(r[32 * part + k1]) * sB, __uint_as_float(r[32 * part + k1 + 1]) * sB, h[e],
-                     l[e]);
+              split2(__uint_as_float(r[32 * part + k1]), __uint_as_float(r[32 * part + k1 + 1]), h[e], l[e]);
             }
-            const uint32_t off = kbase + (uint32_t)(((((cl & 1) * 4 + jj) ^ kr) << 4));
+            const uint32_t off = kbase + (uint32_t)(((((pos & 1) * 4 + jj) ^ kr) << 4));
             sts128(opHi + off, h[0], h[1], h[2], h[3]);
             sts128(opLo + off, l[0], l[1], l[2], l[3]);
           }
@@ -375,31 +417,48 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&opB[gr]);
-      // ---- stage-B epilogue: rows (cl = 4j + q, k1 = lane) of blocks j = 0, 1
-      if (!mix_wait_warp(&accB[gr], par, s_abort) || !mix_wait_warp(&scl[gr], par, s_abort)) {
-        *s_abort = 1;
-        break;
-      }
+      // ---- stage-B epilogue: rows (pencil of position 4j + q, k1 = lane) of
+      // blocks j = 0, 1
+      if (!mix_wait_warp(&accB[gr], par, s_abort)) { *s_abort = 1; break; }
       tc_fence_after();
+      {
+        uint32_t rr[2][32];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int cc = 8 * gr + 4 * j + q;
-        uint32_t rr[32], rc[32];
-        const uint32_t tb_ = tg + (uint32_t)(j * 96);
-        tmem_ld32(tb_, rr);
-        tmem_ld32(tb_ + 32u, rc);
-        tmem_wait_ld();
+        for (int j = 0; j < 2; ++j) {
+          uint32_t rc[32];
+          const uint32_t tb_ = tg + (uint32_t)(j * 96);
+          tmem_ld32(tb_, rr[j]);
+          tmem_ld32(tb_ + 32u, rc);
+          tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 32; ++i) rr[i] = __float_as_uint(__uint_as_float(rr[i]) + __uint_as_float(rc[i]));
-        tmem_ld32(tb_ + 64u, rc);
-        tmem_wait_ld();
+          for (int i = 0; i < 32; ++i) rr[j][i] = __float_as_uint(__uint_as_float(rr[j][i]) + __uint_as_float(rc[i]));
+          tmem_ld32(tb_ + 64u, rc);
+          tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 32; ++i) rr[i] = __float_as_uint(__uint_as_float(rr[i]) + __uint_as_float(rc[i]));
-        const float f = g.out_scale * mix_inv(s_scaleB[cc]);
+          for (int i = 0; i < 32; ++i) rr[j][i] = __float_as_uint(__uint_as_float(rr[j][i]) + __uint_as_float(rc[i]));
+        }
+        // pencils 2q (block 0) and 2q + 1 (block 1): stage-A rows of this
+        // warp's lanes 0-15 and 16-31, whose scale undoes sA / 32 exactly
+        const int cc = 8 * gr + 2 * q;
+        const float f0 = g.out_scale * 32.0f * mix_inv(__shfl_sync(0xffffffffu, sA, 0));
+        const float f1 = g.out_scale * 32.0f * mix_inv(__shfl_sync(0xffffffffu, sA, 16));
+        if constexpr (STRIDED) {
+          // one 16-byte chunk (both columns) per row
 #pragma unroll
-        for (int k2 = 0; k2 < 16; ++k2)
-          sts64(tb + tile_off<STRIDED>(lane + 32 * k2, cc), __uint_as_float(rr[k2]) * f,
-                __uint_as_float(rr[16 + k2]) * f);
+          for (int k2 = 0; k2 < 16; ++k2)
+            sts128(tb + tile_off<STRIDED>(lane + 32 * k2, cc), __float_as_uint(__uint_as_float(rr[0][k2]) * f0),
+                   __float_as_uint(__uint_as_float(rr[0][16 + k2]) * f0),
+                   __float_as_uint(__uint_as_float(rr[1][k2]) * f1),
+                   __float_as_uint(__uint_as_float(rr[1][16 + k2]) * f1));
+        } else {
+#pragma unroll
+          for (int k2 = 0; k2 < 16; ++k2) {
+            sts64(tb + tile_off<STRIDED>(lane + 32 * k2, cc), __uint_as_float(rr[0][k2]) * f0,
+                  __uint_as_float(rr[0][16 + k2]) * f0);
+            sts64(tb + tile_off<STRIDED>(lane + 32 * k2, cc + 1), __uint_as_float(rr[1][k2]) * f1,
+                  __uint_as_float(rr[1][16 + k2]) * f1);
+          }
+        }
       }
       tc_fence_before();
       fence_proxy_async_smem();  // the tile is next read by the store
@@ -474,8 +533,16 @@ __global__ void __launch_bounds__(kMixThreads, 1)
     // ---------------- MMA issuer (warp 9, lane 0) ----------------
     // serves the two groups in the order their operands become ready
     if (lane == 0) {
-      const uint32_t b32h = sb + kMixB32, b32l = b32h + 8192;
-      const uint32_t b16h = sb + kMixB16, b16l = b16h + 4096;
+      // descriptors for K-step 0; a K-step adds its byte offset / 16 to the
+      // start-address field (no carry: every operand lies below 256 KB)
+      const uint64_t dB32h = umma_desc_sw128(sb + kMixB32, 16, 1024), dB32l = umma_desc_sw128(sb + kMixB32 + 8192, 16, 1024);
+      const uint64_t dB16h = umma_desc_sw128(sb + kMixB16, 16, 1024), dB16l = umma_desc_sw128(sb + kMixB16 + 4096, 16, 1024);
+      uint64_t dBh[2], dBl[2];
+      for (int gq = 0; gq < 2; ++gq) {
+        const uint32_t hi = sb + kMixOpA + (uint32_t)gq * 32768u;
+        dBh[gq] = umma_desc_sw128(hi, 4096, 1024);
+        dBl[gq] = umma_desc_sw128(hi + 16384u, 4096, 1024);
+      }
       constexpr uint32_t idA = umma_idesc_f16(128, 64, 0, 0);
       constexpr uint32_t idB = umma_idesc_f16(128, 32, 1, 0);
       const long long ntile = g.ntiles > first ? (g.ntiles - first + step - 1) / step : 0;
@@ -492,19 +559,18 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         for (int gq = 0; gq < 2; ++gq) {
           if (done[gq] >= ntile) continue;
           const uint32_t par = (uint32_t)(done[gq] & 1);
-          const uint32_t opHi = sb + kMixOpA + (uint32_t)gq * 32768u, opLo = opHi + 16384u;
           const uint32_t d = tmem + (uint32_t)gq * 256u;
           if (stage[gq] == 0) {
             if (!mbar_try_wait(&opA[gq], par)) continue;
             tc_fence_after();
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
-              const uint32_t ao = (uint32_t)(s * 32);
-              const uint64_t ah = umma_desc_sw128(opHi + ao, 16, 1024), al = umma_desc_sw128(opLo + ao, 16, 1024);
-              const uint64_t bh = umma_desc_sw128(b32h + s * 32, 16, 1024), bl = umma_desc_sw128(b32l + s * 32, 16, 1024);
-              umma_f16(d + (uint32_t)((s >> 1) * 64), ah, bh, idA, s & 1);  // hi x hi, chains of two
-              umma_f16(d + 128u, al, bh, idA, s > 0);                        // cross terms
-              umma_f16(d + 128u, ah, bl, idA, 1);
+              const uint64_t o = (uint64_t)(2 * s);                // 32 bytes of B
+              const uint32_t ah = d + 192u + (uint32_t)(8 * s);    // 8 columns of A (16 FP16 of K)
+              const uint32_t al = d + 224u + (uint32_t)(8 * s);
+              umma_f16_ts(d + (uint32_t)((s >> 1) * 64), ah, dB32h + o, idA, s & 1);  // hi x hi, chains of two
+              umma_f16_ts(d + 128u, al, dB32h + o, idA, s > 0);                        // cross terms
+              umma_f16_ts(d + 128u, ah, dB32l + o, idA, 1);
             }
             umma_commit(&accA[gq]);
             last_bar[gq] = &accA[gq];
@@ -518,12 +584,11 @@ __global__ void __launch_bounds__(kMixThreads, 1)
               const uint32_t dj = d + (uint32_t)(j * 96);
 #pragma unroll
               for (int s = 0; s < 2; ++s) {
-                const uint32_t ao = (uint32_t)(j * 8192 + s * 2048);
-                const uint64_t ah = umma_desc_sw128(opHi + ao, 4096, 1024), al = umma_desc_sw128(opLo + ao, 4096, 1024);
-                const uint64_t bh = umma_desc_sw128(b16h + s * 32, 16, 1024), bl = umma_desc_sw128(b16l + s * 32, 16, 1024);
-                umma_f16(dj + (uint32_t)(32 * s), ah, bh, idB, 0);  // hi x hi, one K-step each
-                umma_f16(dj + 64u, al, bh, idB, s > 0);             // cross terms
-                umma_f16(dj + 64u, ah, bl, idB, 1);
+                const uint64_t oa = (uint64_t)(j * 512 + s * 128);  // (j * 8192 + s * 2048) bytes
+                const uint64_t ob = (uint64_t)(2 * s);
+                umma_f16(dj + (uint32_t)(32 * s), dBh[gq] + oa, dB16h + ob, idB, 0);  // hi x hi, one K-step each
+                umma_f16(dj + 64u, dBl[gq] + oa, dB16h + ob, idB, s > 0);            // cross terms
+                umma_f16(dj + 64u, dBh[gq] + oa, dB16l + ob, idB, 1);
               }
             }
             umma_commit(&accB[gq]);
@@ -537,7 +602,10 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         if (progressed) {
           t_last = global_ns();
           spins = 0;
-        } else if ((++spins & 255) == 0 && global_ns() - t_last > kWaitNs) {
+          continue;
+        }
+        __nanosleep(20);
+        if ((++spins & 255) == 0 && global_ns() - t_last > kWaitNs) {
           *s_abort = 1;  // neither group handed over operands in time
           break;
         } else if (spins > kWaitLimit) {
