@@ -1,5 +1,8 @@
-// Batches of independent transforms of uneven shapes, replayed as one CUDA
-// graph launch.
+// Batches of independent transforms of uneven shapes.
+//
+// Complex transforms whose axis lengths the persistent batch kernel runs
+// (batch_pass.cuh) execute as ONE launch of that kernel over a work list of
+// every axis pass of every transform.  Other batches replay one CUDA graph:
 //
 // A batch holds N plans (any shapes, kinds and precisions).  The first
 // execute with a given set of buffers captures every plan's passes into a
@@ -16,6 +19,7 @@
 #include <cstring>
 #include <mutex>
 #include <vector>
+#include "batch_pass.h"
 #include "batch_rule.h"
 #include "dfft.h"
 #include "dfft_plan.h"
@@ -35,6 +39,7 @@ struct Batch {
   cudaEvent_t fork = nullptr;
   cudaEvent_t join[kBatchStreams] = {};
   int launches = 0;
+  std::unique_ptr<PersistentBatch> persist;  // the one-launch form, when it serves the batch
   std::mutex mu;
   ~Batch() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -98,7 +103,7 @@ static void capture(Batch* B, const void* const* ins, void* const* outs, cudaGra
   cuda_check(err, "cudaStreamEndCapture");
 }
 
-Batch* build_batch(int n, const dfft_plan* plans) {
+Batch* build_batch(int n, const dfft_plan* plans, unsigned flags) {
   if (n < 1 || !plans) throw Error{DFFT_ERROR_INVALID_VALUE, "a batch needs at least one plan"};
   std::unique_ptr<Batch> B(new Batch());
   cuda_check(cudaGetDevice(&B->device), "cudaGetDevice");
@@ -108,6 +113,20 @@ Batch* build_batch(int n, const dfft_plan* plans) {
       throw Error{DFFT_ERROR_INVALID_VALUE, "every plan of a batch must live on the current device"};
     B->plans.push_back(plans[i]->impl);
     B->launches += (int)plans[i]->impl->passes.size();
+  }
+  if (!(flags & DFFT_BATCH_GRAPH)) {
+    // a pass is claimed about `lag` transforms after the one it depends on:
+    // half the graph's branch count (transforms whose buffers fit L2 at once)
+    double total = 0;
+    for (const Plan* p : B->plans) total += (double)(p->in_bytes() + p->out_bytes());
+    int l2 = 0;
+    if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, B->device) != cudaSuccess) {
+      cudaGetLastError();
+      l2 = 0;
+    }
+    const int lag = batch_branch_rule(n, total, l2, kBatchStreams) / 2;
+    B->persist = make_persistent_batch(B->plans, lag < 1 ? 1 : lag);
+    if (B->persist) B->launches = 1;
   }
   for (auto& s : B->side) cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
   cuda_check(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -125,6 +144,16 @@ void execute_batch(Batch* B, const void* const* ins, void* const* outs, cudaStre
   int cur = -1;
   cuda_check(cudaGetDevice(&cur), "cudaGetDevice");
   if (cur != B->device) cuda_check(cudaSetDevice(B->device), "cudaSetDevice");
+  if (B->persist) {
+    try {
+      launch_persistent_batch(B->persist.get(), ins, outs, s);
+    } catch (...) {
+      if (cur != B->device) cudaSetDevice(cur);
+      throw;
+    }
+    if (cur != B->device) cudaSetDevice(cur);
+    return;
+  }
   bool same = B->exec && (int)B->last_in.size() == n;
   for (int i = 0; same && i < n; ++i) same = B->last_in[i] == ins[i] && B->last_out[i] == outs[i];
   if (!same) {
@@ -164,10 +193,14 @@ using dfft::Error;
 extern "C" {
 
 int dfft_batch_create(dfft_batch* batch, int nplans, const dfft_plan* plans) {
+  return dfft_batch_create_ex(batch, nplans, plans, 0u);
+}
+
+int dfft_batch_create_ex(dfft_batch* batch, int nplans, const dfft_plan* plans, unsigned flags) {
   try {
     if (!batch) throw Error{DFFT_ERROR_INVALID_VALUE, "batch is NULL"};
     *batch = nullptr;
-    *batch = new dfft_batch_s{dfft::build_batch(nplans, plans)};
+    *batch = new dfft_batch_s{dfft::build_batch(nplans, plans, flags)};
     return DFFT_SUCCESS;
   } catch (const Error& e) {
     dfft::set_error(e.msg);

@@ -225,6 +225,18 @@ __device__ __forceinline__ bool mix_wait(uint64_t* bar, uint32_t parity, volatil
   }
   return false;
 }
+// Non-blocking test of a phase (try_wait may park the thread for a while,
+// which a poller of several barriers cannot afford).
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
 // The same wait with a warp-uniform result (every lane waits; the warp
 // proceeds only if all lanes saw the phase complete), so that the
 // .sync.aligned tensor-memory loads after it run converged.
@@ -561,7 +573,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
           const uint32_t par = (uint32_t)(done[gq] & 1);
           const uint32_t d = tmem + (uint32_t)gq * 256u;
           if (stage[gq] == 0) {
-            if (!mbar_try_wait(&opA[gq], par)) continue;
+            if (!mbar_test(&opA[gq], par)) continue;
             tc_fence_after();
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
@@ -577,7 +589,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
             last_par[gq] = par;
             stage[gq] = 1;
           } else {
-            if (!mbar_try_wait(&opB[gq], par)) continue;
+            if (!mbar_test(&opB[gq], par)) continue;
             tc_fence_after();
 #pragma unroll
             for (int j = 0; j < 2; ++j) {

@@ -40,7 +40,7 @@ namespace dfft {
 constexpr int kTmaBufs = 3;
 constexpr unsigned kWaitLimit = 1u << 26;    // try_wait rounds before giving up
 constexpr uint64_t kWaitNs = 2000000000ull;  // and at most ~2 s of wall time
-enum : int { DFFT_DEVERR_TMA_TIMEOUT = 1, DFFT_DEVERR_TMA_ALIGN = 2 };
+enum : int { DFFT_DEVERR_TMA_TIMEOUT = 1, DFFT_DEVERR_TMA_ALIGN = 2, DFFT_DEVERR_BATCH_ITEM = 3 };
 
 struct TmaGeom {
   int C;              // columns (strided) or pencils (contiguous) per tile

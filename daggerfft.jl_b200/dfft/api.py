@@ -408,18 +408,20 @@ def ifft_(A, decomp=None, dims=(1, 2, 3), method="plain"):
 
 
 class Batch:
-    """Independent plans executed together as one CUDA graph launch
-    (``dfft_batch_*``).  ``execute(ins, outs)`` takes one input and one
-    output tensor per plan; the graph is captured on the first call and
-    replayed while the same buffers are passed."""
+    """Independent plans executed together (``dfft_batch_*``): one launch of
+    the persistent batch kernel when every plan is a complex transform of
+    the lengths it runs (``launches == 1``), otherwise one CUDA graph of the
+    plans' passes (``graph=True`` forces the graph).  ``execute(ins, outs)``
+    takes one input and one output tensor per plan; a graph is captured on
+    the first call and replayed while the same buffers are passed."""
 
-    def __init__(self, plans: Sequence[Plan]):
+    def __init__(self, plans: Sequence[Plan], graph: bool = False):
         L = _lib.lib()
         self._L = L
         self.plans = list(plans)  # keeps the plans alive
-        L.dfft_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
-                                        ctypes.POINTER(ctypes.c_void_p)]
-        L.dfft_batch_create.restype = ctypes.c_int
+        L.dfft_batch_create_ex.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint]
+        L.dfft_batch_create_ex.restype = ctypes.c_int
         L.dfft_batch_execute.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
                                          ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]
         L.dfft_batch_execute.restype = ctypes.c_int
@@ -429,7 +431,7 @@ class Batch:
         L.dfft_batch_destroy.restype = ctypes.c_int
         arr = (ctypes.c_void_p * len(self.plans))(*[p._h.value for p in self.plans])
         h = ctypes.c_void_p()
-        check(L.dfft_batch_create(ctypes.byref(h), len(self.plans), arr))
+        check(L.dfft_batch_create_ex(ctypes.byref(h), len(self.plans), arr, 1 if graph else 0))
         self._h = h
         n = ctypes.c_int()
         check(L.dfft_batch_launches(h, ctypes.byref(n)))

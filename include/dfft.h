@@ -71,9 +71,12 @@ typedef enum { DFFT_F32 = 0, DFFT_F64 = 1 } dfft_precision;
 /* decomposition tags (src/fft.jl:13-15) */
 typedef enum { DFFT_PENCIL = 0, DFFT_SLAB = 1 } dfft_decomp;
 
-/* arithmetic form: PLAIN = FP32/FP64 CUDA-core Stockham; MIXED (reserved: the
- * tensor-core form is not built in this version, plans return an error) = tensor-core
- * radix-16/32 stages with FP16 hi+lo split products (ComplexF32 only) */
+/* arithmetic form: PLAIN = FP32/FP64 CUDA-core Stockham; MIXED = ComplexF32
+ * axes of length 512 as radix-32 x radix-16 complex matrix products on the
+ * tensor cores (tcgen05, FP16 hi+lo split operands, FP32 accumulation,
+ * per-pencil power-of-two scaling; relative L2 error ~3e-7 per 3-D
+ * transform); other axes, ComplexF64 and FFT/IFFT of other lengths run the
+ * plain form; real and r2r transforms return DFFT_ERROR_INVALID_VALUE */
 typedef enum { DFFT_PLAIN = 0, DFFT_MIXED = 1 } dfft_method;
 
 /* FFTW r2r kinds (fftw_r2r_kind values; src/fft.jl:1-11) */
@@ -145,9 +148,11 @@ DFFT_API int dfft_plan_destroy(dfft_plan plan);
 /*
  * Reads and clears the device error word of the current device.  Kernels
  * whose bounded waits expire (TMA tile pipeline) record a non-zero code there
- * instead of hanging or faulting: 1 = a tile load did not complete in time,
- * 2 = a tile buffer was not aligned for the bulk copies (nothing was
- * issued).  Synchronises the device.
+ * instead of hanging or faulting: 1 = a tile load or a dependency did not
+ * complete in time, 2 = a tile buffer was not aligned for the bulk copies
+ * (nothing was issued), 3 = a batch work item of a length the persistent
+ * kernel does not run (nothing was computed for it).  Synchronises the
+ * device.
  */
 DFFT_API int dfft_device_error(int* code);
 
@@ -166,14 +171,23 @@ DFFT_API int dfft_wisdom_size(int* n);
 /* ---- batches of uneven transforms -----------------------------------
  *
  * No counterpart in the reference (north-star addition): N independent
- * plans (any shapes/kinds) executed as one CUDA graph launch.  The first
- * execute with a set of buffers captures every plan's passes as concurrent
- * branches; later executes with the same buffers replay the graph, new
- * buffers update it.  Plans must outlive the batch and live on the current
- * device.
+ * plans (any shapes/kinds) executed together.  When every plan is a complex
+ * transform (FFT / IFFT, one precision) whose axis lengths the persistent
+ * batch kernel runs (16, 24, 32, 40, 48, 60, 64, 72, 80, 96, 100, 120, 128,
+ * 144, 160, 192, 256), the batch is ONE kernel launch over a work list of
+ * every axis pass of every transform (passes of one transform run in its
+ * stage order; a pass waits, bounded, for its predecessor).  Otherwise the
+ * first execute with a set of buffers captures every plan's passes as
+ * concurrent branches of a CUDA graph; later executes with the same buffers
+ * replay the graph, new buffers update it.  Plans must outlive the batch and
+ * live on the current device.  dfft_batch_launches reports which: 1 for the
+ * persistent kernel, else the graph's kernel count.
  */
 typedef struct dfft_batch_s* dfft_batch;
+enum { DFFT_BATCH_GRAPH = 1u << 0 /* always the graph of the plans' own passes */ };
 DFFT_API int dfft_batch_create(dfft_batch* batch, int nplans, const dfft_plan* plans);
+/* The same with flags (DFFT_BATCH_GRAPH). */
+DFFT_API int dfft_batch_create_ex(dfft_batch* batch, int nplans, const dfft_plan* plans, unsigned flags);
 DFFT_API int dfft_batch_execute(dfft_batch batch, const void* const* ins, void* const* outs,
                                 void* stream);
 DFFT_API int dfft_batch_launches(dfft_batch batch, int* launches);

@@ -20,14 +20,18 @@ def _grids(n, seed=0):
     return [tuple(int(e) for e in rng.choice(EDGES, 3)) for _ in range(n)]
 
 
-def test_batch_uneven_grids_match_oracle_and_alone():
+@pytest.mark.parametrize("graph", [False, True])
+def test_batch_uneven_grids_match_oracle_and_alone(graph):
+    # graph=False: one launch of the persistent batch kernel (these lengths
+    # are all in its set); graph=True: the graph of the plans' own passes,
+    # bit-identical to each plan run alone
     shapes = _grids(12, seed=1)
     arrays = [rand(s, np.complex64, seed=i, kind="uniform11") for i, s in enumerate(shapes)]
     ins = [to_gpu(a) for a in arrays]
     plans = [dfft.gpu_plan_transform(dfft.FFT(), g, (1, 2, 3), flags=dfft.FLAG_TUNE) for g in ins]
     outs = [dfft.empty_like_layout(p.out_shape, g.dtype, g) for p, g in zip(plans, ins)]
-    b = dfft.Batch(plans)
-    assert b.launches == sum(p.launches for p in plans)
+    b = dfft.Batch(plans, graph=graph)
+    assert b.launches == (sum(p.launches for p in plans) if graph else 1)
     for rep in range(3):  # capture, then replays of the same graph
         b.execute(ins, outs)
         torch.cuda.synchronize()
@@ -35,7 +39,10 @@ def test_batch_uneven_grids_match_oracle_and_alone():
             assert rel(to_np(o), oracle.fft(a, dims=(1, 2, 3))) <= 1e-5
             alone = dfft.empty_like_layout(p.out_shape, g.dtype, g)
             p.execute(g, alone)
-            assert torch.equal(alone, o), "batched result differs from the plan run alone"
+            if graph:
+                assert torch.equal(alone, o), "batched result differs from the plan run alone"
+            else:  # other kernels than the plan's: equal to rounding
+                assert rel(to_np(o), to_np(alone)) <= 1e-6
     # new buffers: the graph is updated, results follow the new inputs
     ins2 = [to_gpu(rand(s, np.complex64, seed=100 + i)) for i, s in enumerate(shapes)]
     b.execute(ins2, outs)
@@ -59,3 +66,34 @@ def test_batch_mixes_kinds_and_precisions():
     assert rel(to_np(outs[0]), oracle.ifft(a, dims=(1, 2, 3))) <= 1e-5
     assert rel(to_np(outs[1]), oracle.rfft(r, dims=(1, 2))) <= 1e-12
     assert rel(to_np(outs[2]), oracle.fft(d, dims=(1, 2), transforms=(oracle.R2R((oracle.REDFT10, oracle.REDFT10)),))) <= 1e-12
+
+
+def test_persistent_batch_inverse_and_float64():
+    # inverse transforms (reverse stage order, 1/N) and ComplexF64, 2-D and 3-D
+    shapes = [(48, 64, 40), (96, 24), (160, 120, 16), (32, 256, 16)]
+    for dt, tol in ((np.complex64, 1e-5), (np.complex128, 1e-12)):
+        arrays = [rand(s, dt, seed=7 + i) for i, s in enumerate(shapes)]
+        ins = [to_gpu(a) for a in arrays]
+        plans = [dfft.gpu_plan_transform(dfft.IFFT(), g, tuple(range(1, g.dim() + 1))) for g in ins]
+        outs = [dfft.empty_like_layout(p.out_shape, g.dtype, g) for p, g in zip(plans, ins)]
+        b = dfft.Batch(plans)
+        assert b.launches == 1
+        for _ in range(2):
+            b.execute(ins, outs)
+            torch.cuda.synchronize()
+            for a, o in zip(arrays, outs):
+                assert rel(to_np(o), oracle.ifft(a, dims=tuple(range(1, a.ndim + 1)))) <= tol
+    assert dfft.device_error() == 0
+
+
+def test_persistent_batch_falls_back_to_graph():
+    # a length outside the persistent kernel's set (7 * 11): the graph form
+    a = rand((77, 32, 8), np.complex64, seed=1)
+    g = to_gpu(a)
+    p = dfft.gpu_plan_transform(dfft.FFT(), g, (1, 2, 3))
+    b = dfft.Batch([p])
+    assert b.launches == p.launches
+    o = dfft.empty_like_layout(p.out_shape, g.dtype, g)
+    b.execute([g], [o])
+    torch.cuda.synchronize()
+    assert rel(to_np(o), oracle.fft(a, dims=(1, 2, 3))) <= 1e-5
