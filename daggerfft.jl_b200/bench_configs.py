@@ -170,14 +170,22 @@ def c4():
            for s in shapes]
     plans = [dfft.gpu_plan_transform(dfft.FFT(), x, (1, 2, 3), flags=dfft.FLAG_TUNE) for x in ins]
     outs = [dfft.empty_like_layout(p.out_shape, x.dtype, x) for p, x in zip(plans, ins)]
-    batch = dfft.Batch(plans)                 # the persistent kernel: one launch
-    graph = dfft.Batch(plans, graph=True)     # the graph of the plans' own passes
-    ms_batch = timed(lambda: batch.execute(ins, outs))
+    graph = dfft.Batch(plans)                     # the graph of the plans' own passes
+    persist = dfft.Batch(plans, persistent=True)  # the persistent kernel: one launch
     ms_graph = timed(lambda: graph.execute(ins, outs))
+    ms_persist = timed(lambda: persist.execute(ins, outs))
+    by_lag = {}
+    for lag in (1, 4, 16, 64):
+        b = dfft.Batch(plans, persistent=True, lag=lag)
+        by_lag[str(lag)] = round(timed(lambda: b.execute(ins, outs)), 4)
+        del b
     ms_seq = timed(lambda: [p.execute(x, o) for p, x, o in zip(plans, ins, outs)])
-    batch.execute(ins, outs)
+    persist.execute(ins, outs)
     torch.cuda.synchronize()
     fx = sfft()
+    err_p = max(hrel(host(o), fx.fftn(host(x), workers=WORKERS)) for x, o in zip(ins, outs))
+    graph.execute(ins, outs)
+    torch.cuda.synchronize()
     err = max(hrel(host(o), fx.fftn(host(x), workers=WORKERS)) for x, o in zip(ins, outs))
     elems = sum(a * b * c for a, b, c in shapes)
     byts = 3 * 2 * elems * 8
@@ -194,14 +202,17 @@ def c4():
     dbytes = 2 * 2 * 2 * 256 * 256 * 32 * 8
     d, Eh, Rh = host(D), host(E), host(R)
     # scipy's unnormalised DCT-II / DCT-III are FFTW's REDFT10 / REDFT01
-    return {"config": "c4 64 uneven C2C ComplexF32 grids as one persistent-kernel launch; DCT-II/III Float64 256x256x32",
-            "grids": len(shapes), "elements": elems, "kernel_launches": batch.launches,
-            "ms_batch": round(ms_batch, 4), "GBps_batch": round(byts / ms_batch / 1e6, 1),
-            "kernel_launches_in_graph_form": graph.launches,
-            "ms_graph": round(ms_graph, 4), "ms_sequential_launches": round(ms_seq, 4),
-            "GBps_graph": round(byts / ms_graph / 1e6, 1),
+    return {"config": "c4 64 uneven C2C ComplexF32 grids as one graph launch (and as one persistent-kernel launch); DCT-II/III Float64 256x256x32",
+            "grids": len(shapes), "elements": elems,
+            "kernel_launches_in_graph": graph.launches,
+            "ms_graph": round(ms_graph, 4), "GBps_graph": round(byts / ms_graph / 1e6, 1),
+            "persistent_kernel_launches": persist.launches,
+            "ms_persistent": round(ms_persist, 4), "GBps_persistent": round(byts / ms_persist / 1e6, 1),
+            "ms_persistent_by_lag": by_lag,
+            "ms_sequential_launches": round(ms_seq, 4),
             "GBps_sequential": round(byts / ms_seq / 1e6, 1),
             "grids_worst_fwd_rel_l2_vs_host_fp64": err,
+            "grids_worst_fwd_rel_l2_vs_host_fp64_persistent": err_p,
             "dct2_dct3_256x256x32_f64_ms": round(ms_dct, 4),
             "dct_GBps": round(dbytes / ms_dct / 1e6, 1),
             "dct2_rel_l2_vs_host_fp64": hrel(Eh, fx.dctn(d, type=2, axes=(0, 1), workers=WORKERS)),

@@ -46,7 +46,9 @@ enum IoKind : int {
   IO_HERM_PAIR = 3,  // load only: even-length C2R pre-pass (real length 2n)
   IO_HERM_FULL = 4,  // load only: odd-length C2R, Hermitian mirror
   IO_TRUNC = 5,      // store only: complex, keep k <= n
-  IO_R2R = 6         // FFTW r2r kind `r2r` on real data of extent n
+  IO_R2R = 6,        // FFTW r2r kind `r2r` on real data of extent n
+  IO_CPLX_TW = 7     // store only: complex times w[(j * k) mod n], j = (b mod t_ia) / t_i
+                     // (the twiddle between the two passes of a four-step axis)
 };
 
 // FFTW r2r kind numbers (fftw_r2r_kind).
@@ -66,7 +68,21 @@ struct IoAny {
   const void* chirp;
   const void* mul;
   int chirp_n;
+  // Two-level column split of the outer index (four-step output): with
+  // o1 > 0 the column base is (qo mod o1) * so + (qo / o1) * so2.
+  long long o1, so2;
+  // Sub-axis of a four-step pair: the column at base b holds elements
+  // j + t_m * k of the whole axis, j = (b mod t_ia) / t_i.  IO_CPLX_TW
+  // multiplies by w[(j * k) mod n]; with t_m > 0 the chirp and mul tables
+  // are indexed by j + t_m * k (Bluestein around a four-step pair).
+  long long t_i, t_ia;
+  int t_m;
 };
+
+// Column base of side `io` for the outer column index qo.
+__host__ __device__ __forceinline__ long long io_outer(const IoAny& io, long long qo) {
+  return io.o1 > 0 ? (qo % io.o1) * io.so + (qo / io.o1) * io.so2 : qo * io.so;
+}
 
 struct PassDesc {
   int L;                    // transform length of this pass
@@ -239,6 +255,13 @@ __device__ __forceinline__ void store_raw(const IoAny& io, long long b, int k,
     case IO_TRUNC:
       if (k <= io.n) reinterpret_cast<V*>(io.p)[b + k * io.sk] = cscale(v, s);
       return;
+    case IO_CPLX_TW: {
+      const long long j = (b % io.t_ia) / io.t_i;
+      const V w = ldg_c(reinterpret_cast<const V*>(io.w) +
+                        (long long)(((unsigned long long)j * (unsigned long long)k) % (unsigned long long)io.n));
+      reinterpret_cast<V*>(io.p)[b + k * io.sk] = cscale(cmul(v, w), s);
+      return;
+    }
     case IO_REAL_PAIR: {
       T* p = reinterpret_cast<T*>(io.p);
       if (io.sk == 1) { *reinterpret_cast<V*>(p + b + 2 * (long long)k) = cscale(v, s); return; }
@@ -267,16 +290,22 @@ __device__ __forceinline__ void store_raw(const IoAny& io, long long b, int k,
   }
 }
 
+// Index along the whole axis of element k of the column at base b.
+__device__ __forceinline__ long long axis_index(const IoAny& io, long long b, int k) {
+  return io.t_m > 0 ? (b % io.t_ia) / io.t_i + (long long)io.t_m * k : (long long)k;
+}
+
 // Element access with the optional Bluestein chirp / filter multiply.
 template <typename T>
 __device__ __forceinline__ typename cvec<T>::type load_elem(const IoAny& io, long long b, int k) {
   typedef typename cvec<T>::type V;
   if (io.chirp) {
-    if (k >= io.chirp_n) return mk<V>((T)0, (T)0);
-    return cmul(load_raw<T>(io, b, k), ldg_c(reinterpret_cast<const V*>(io.chirp) + k));
+    const long long n = axis_index(io, b, k);
+    if (n >= io.chirp_n) return mk<V>((T)0, (T)0);
+    return cmul(load_raw<T>(io, b, k), ldg_c(reinterpret_cast<const V*>(io.chirp) + n));
   }
   V v = load_raw<T>(io, b, k);
-  if (io.mul) v = cmul(v, ldg_c(reinterpret_cast<const V*>(io.mul) + k));
+  if (io.mul) v = cmul(v, ldg_c(reinterpret_cast<const V*>(io.mul) + axis_index(io, b, k)));
   return v;
 }
 
@@ -285,8 +314,9 @@ __device__ __forceinline__ void store_elem(const IoAny& io, long long b, int k,
                                            typename cvec<T>::type v, T s) {
   typedef typename cvec<T>::type V;
   if (io.chirp) {
-    if (k >= io.chirp_n) return;
-    v = cmul(v, ldg_c(reinterpret_cast<const V*>(io.chirp) + k));
+    const long long n = axis_index(io, b, k);
+    if (n >= io.chirp_n) return;
+    v = cmul(v, ldg_c(reinterpret_cast<const V*>(io.chirp) + n));
   }
   store_raw<T>(io, b, k, v, s);
 }
@@ -476,8 +506,8 @@ __device__ __forceinline__ ColCtx col_ctx(const PassDesc& d, int P) {
   x.cv = q < d.Q;
   const long long qi = x.cv ? q % d.I : 0;
   const long long qo = x.cv ? q / d.I : 0;
-  x.ib = qi * d.in.si + qo * d.in.so;
-  x.ob = qi * d.out.si + qo * d.out.so;
+  x.ib = qi * d.in.si + io_outer(d.in, qo);
+  x.ob = qi * d.out.si + io_outer(d.out, qo);
   return x;
 }
 

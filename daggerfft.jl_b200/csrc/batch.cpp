@@ -1,8 +1,9 @@
 // Batches of independent transforms of uneven shapes.
 //
-// Complex transforms whose axis lengths the persistent batch kernel runs
-// (batch_pass.cuh) execute as ONE launch of that kernel over a work list of
-// every axis pass of every transform.  Other batches replay one CUDA graph:
+// With DFFT_BATCH_PERSISTENT, complex transforms whose axis lengths the
+// persistent batch kernel runs (batch_pass.cuh) execute as ONE launch of
+// that kernel over a work list of every axis pass of every transform.  By
+// default (and for other batches) the batch replays one CUDA graph:
 //
 // A batch holds N plans (any shapes, kinds and precisions).  The first
 // execute with a given set of buffers captures every plan's passes into a
@@ -114,9 +115,11 @@ Batch* build_batch(int n, const dfft_plan* plans, unsigned flags) {
     B->plans.push_back(plans[i]->impl);
     B->launches += (int)plans[i]->impl->passes.size();
   }
-  if (!(flags & DFFT_BATCH_GRAPH)) {
+  if ((flags & DFFT_BATCH_PERSISTENT) && !(flags & DFFT_BATCH_GRAPH)) {
     // a pass is claimed about `lag` transforms after the one it depends on:
-    // half the graph's branch count (transforms whose buffers fit L2 at once)
+    // the caller's (flag bits 8-15), else half the graph's branch count
+    // (transforms whose buffers fit L2 at once)
+    const int user_lag = (int)((flags >> 8) & 0xFFu);
     double total = 0;
     for (const Plan* p : B->plans) total += (double)(p->in_bytes() + p->out_bytes());
     int l2 = 0;
@@ -124,7 +127,7 @@ Batch* build_batch(int n, const dfft_plan* plans, unsigned flags) {
       cudaGetLastError();
       l2 = 0;
     }
-    const int lag = batch_branch_rule(n, total, l2, kBatchStreams) / 2;
+    const int lag = user_lag > 0 ? user_lag : batch_branch_rule(n, total, l2, kBatchStreams) / 2;
     B->persist = make_persistent_batch(B->plans, lag < 1 ? 1 : lag);
     if (B->persist) B->launches = 1;
   }

@@ -75,8 +75,8 @@ __device__ __noinline__ void batch_tile(const PassDesc& d, long long item, unsig
     const bool cv = active && q < d.Q;
     const long long qi = cv ? q % d.I : 0;
     const long long qo = cv ? q / d.I : 0;
-    const long long ib = qi * d.in.si + qo * d.in.so;
-    const long long ob = qi * d.out.si + qo * d.out.so;
+    const long long ib = qi * d.in.si + io_outer(d.in, qo);
+    const long long ob = qi * d.out.si + io_outer(d.out, qo);
     static_stages<T, L, P, true, 0, 0, 0, 1, 1, 0, PadCol<V>, PadCol<V>, PadCol<V>, GlobalTw<V>, Rs...>(
         d, t, col, col, col, tw, ib, ob, cv);
   }

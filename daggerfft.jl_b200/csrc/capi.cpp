@@ -87,9 +87,11 @@ int dfft_plan_describe(dfft_plan plan, char* buf, size_t len) {
       for (int i = 0; i < q.d.nst; ++i) rad += (i ? "x" : "") + std::to_string(q.d.radix[i]);
       if (q.mixed) rad = "32x16(tcgen05 fp16 hi+lo)";
       char line[256];
-      std::snprintf(line, sizeof line, "%s L=%d I=%lld O=%lld grid=%u block=%u smem=%zu radices=%s\n", kind,
+      // the two passes of a four-step axis: twiddled store, then the split output
+      const char* step = q.d.out.kind == dfft::IO_CPLX_TW ? " four-step=1" : q.d.out.o1 > 0 ? " four-step=2" : "";
+      std::snprintf(line, sizeof line, "%s L=%d I=%lld O=%lld grid=%u block=%u smem=%zu radices=%s%s\n", kind,
                     q.d.L, q.d.I, q.d.I > 0 ? q.d.Q / q.d.I : 0LL, q.grid.x, q.block.x, q.smem,
-                    rad.empty() ? "-" : rad.c_str());
+                    rad.empty() ? "-" : rad.c_str(), step);
       out += line;
     }
     const size_t n = out.size() < len - 1 ? out.size() : len - 1;

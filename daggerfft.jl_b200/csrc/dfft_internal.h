@@ -44,6 +44,7 @@ struct Pass {
   dim3 grid, block;
   size_t smem = 0;
   int src = BUF_IN, dst = BUF_OUT;
+  size_t src_off = 0, dst_off = 0;  // byte offsets into those buffers
   bool is_static = false;
   // persistent pipelined pass (bulk copies); tma: strided, tensor
   // {I*xscale, L, O} of 8-byte elements

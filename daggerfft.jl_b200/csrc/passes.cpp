@@ -1089,7 +1089,152 @@ cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream,
 namespace dfft {
 
 // ---------------------------------------------------------------------------
-// Bluestein (chirp-z) for lengths no single-pass kernel handles.
+// Four-step decomposition of a complex axis that no single pass handles:
+// L = L1 * L2, n = n1 + L1 n2, k = k2 + L2 k1,
+//   X[k2 + L2 k1] = sum_n1 W_L1^(n1 k1) [ W_L^(n1 k2) sum_n2 x[n1 + L1 n2] W_L2^(n2 k2) ].
+// Pass A: L2-point transforms along the sub-axis of stride I*L1 (columns
+// (i, n1, o)), into a scratch in the same layout, times W_L^(n1 k2) on the
+// way out; pass B: L1-point transforms along stride I (columns (i, k2, o)),
+// written to position k2 + L2 k1 (the output's two-level column split).
+// Each factor runs as one pass: a static plan, or the dynamic kernel for
+// lengths up to 4096 with prime factors up to 13 that fit one CTA.  Splits
+// with two static factors come first, then the most balanced one.
+// ---------------------------------------------------------------------------
+
+static int four_step_factor(int dbl, int n) {
+  const StaticPlan* sp = find_static(dbl, n);
+  if (sp && sp->P <= sp->lb) return VARIANT_DIRECT;
+  if (n > 4096) return 0;
+  const std::vector<int> rad = dynamic_radices(n);
+  if (rad.empty() || (int)rad.size() > kMaxStages) return 0;
+  int P = 1;
+  for (int R : rad) {
+    const int B = 16 / R;
+    const int need = (n / R + B - 1) / B;
+    if (need > P) P = need;
+  }
+  return P <= 1024 ? VARIANT_DYNAMIC : 0;
+}
+
+static bool four_step_split(int dbl, int L, int* L1, int* L2) {
+  int best = 0, best_static = 0;
+  for (int d = 2; (long long)d * d <= L; ++d) {
+    if (L % d != 0) continue;
+    const int va = four_step_factor(dbl, d), vb = four_step_factor(dbl, L / d);
+    if (!va || !vb) continue;
+    const int st = va == VARIANT_DIRECT && vb == VARIANT_DIRECT;
+    if (st >= best_static) {
+      best = d;
+      best_static = st;
+    }
+  }
+  if (!best) return false;
+  *L1 = best;
+  *L2 = L / best;
+  return true;
+}
+
+// The pass pair of a four-step transform of length s.L = L1 * L2 along a
+// complex axis with unit inner stride (element (i, n, o) at i + n I + o so).
+// Pass A reads s.in (its chirp / mul indexed along the whole axis) and
+// writes the scratch (I, L, O) times the twiddle; pass B reads the scratch
+// and writes s.out at k2 + L2 k1 (with its chirp and the scale).
+static void four_step_pair(const PassSpec& s, int L1, int L2, Pass* pa, Pass* pb) {
+  const long long L = (long long)L1 * L2;
+  auto tw = twiddle_table(s.dbl, L, 1, 0, (int)L, s.inverse != 0);
+  PassSpec a = s;
+  a.L = L2;
+  a.I = s.I * L1;
+  a.O = s.O;
+  a.scale = 1.0;
+  a.fast_io = false;
+  a.epi = false;
+  a.C = 0;
+  a.variant = four_step_factor(s.dbl, L2);
+  a.in.sk = s.I * L1;  // si = 1 and so as for the whole axis
+  // sub-axis index j from the column base b = i + j I + o so: (b mod so) / I
+  // (so need not be a multiple of I L1: Bluestein's input has L < L1 L2 rows)
+  if (a.in.chirp || a.in.mul) {
+    a.in.t_i = s.I;
+    a.in.t_ia = a.in.so;
+    a.in.t_m = L1;
+  }
+  a.out = IoAny{};
+  a.out.kind = IO_CPLX_TW;
+  a.out.si = 1;
+  a.out.so = s.I * L;
+  a.out.sk = s.I * L1;
+  a.out.w = tw->p;
+  a.out.n = (int)L;
+  a.out.t_i = s.I;
+  a.out.t_ia = s.I * L;
+  a.keep.push_back(tw);
+  PassSpec b = s;
+  b.L = L1;
+  b.I = s.I;
+  b.O = (long long)L2 * s.O;
+  b.fast_io = !s.out.chirp;
+  b.epi = false;
+  b.C = 0;
+  b.variant = four_step_factor(s.dbl, L1);
+  b.in = IoAny{};
+  b.in.kind = IO_CPLX;
+  b.in.si = 1;
+  b.in.so = s.I * L1;
+  b.in.sk = s.I;
+  b.out.sk = s.I * L2;
+  b.out.so = s.I;
+  b.out.o1 = L2;
+  b.out.so2 = s.out.so;
+  if (b.out.chirp) {
+    b.out.t_i = s.I;
+    b.out.t_ia = s.out.so;
+    b.out.t_m = L2;
+  }
+  *pa = make_pass(a);
+  *pb = make_pass(b);
+}
+
+static bool plain_complex_axis(const PassSpec& s) {
+  const long long L = s.L;
+  return s.in.kind == IO_CPLX && s.out.kind == IO_CPLX && !s.epi && !s.in.chirp && !s.out.chirp &&
+         !s.in.mul && s.in.o1 == 0 && s.out.o1 == 0 && s.in.si == 1 && s.out.si == 1 && s.in.sk == s.I &&
+         s.out.sk == s.I && s.in.so == s.I * L && s.out.so == s.I * L;
+}
+
+static size_t add_four_step(std::vector<Pass>& out, const PassSpec& s, int L1, int L2, int src, int dst) {
+  Pass pa, pb;
+  four_step_pair(s, L1, L2, &pa, &pb);
+  pa.src = src;
+  pa.dst = BUF_CHIRP;
+  pb.src = BUF_CHIRP;
+  pb.dst = dst;
+  out.push_back(std::move(pa));
+  out.push_back(std::move(pb));
+  return (size_t)(s.I * s.O) * (size_t)s.L * (s.dbl ? 16 : 8);
+}
+
+// One pass, or a four-step pair, for a plain complex axis; no Bluestein.
+// Returns the scratch bytes (BUF_CHIRP) the passes need.
+static size_t add_direct_passes(std::vector<Pass>& out, const PassSpec& s, unsigned flags, int src, int dst) {
+  try {
+    Pass p = plan_pass(s, flags);
+    p.src = src;
+    p.dst = dst;
+    out.push_back(std::move(p));
+    return 0;
+  } catch (const Error& e) {
+    if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
+  }
+  int L1 = 0, L2 = 0;
+  if (!plain_complex_axis(s) || !four_step_split(s.dbl, s.L, &L1, &L2))
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE,
+                "length " + std::to_string(s.L) + " has no single-pass or four-step form"};
+  return add_four_step(out, s, L1, L2, src, dst);
+}
+
+// ---------------------------------------------------------------------------
+// Bluestein (chirp-z) for lengths no single pass or four-step pair handles.
 //   X_k = w_k sum_n (x_n w_n) b_{k-n},  w_n = exp(s i pi n^2 / L),
 //   b_m = conj(w_m), s = -1 (forward) or +1 (inverse);
 // the convolution runs as FFT_M, a pointwise multiply by
@@ -1162,6 +1307,7 @@ static BluesteinTables bluestein_tables(int dbl, int L, int sgn) {
     }
   }
   void* dB = nullptr;
+  void* dS = nullptr;
   cuda_check(cudaMalloc(&dB, B.size() * sizeof(double)), "cudaMalloc(bluestein B)");
   std::vector<double> F(B.size());
   try {
@@ -1176,21 +1322,23 @@ static BluesteinTables bluestein_tables(int dbl, int L, int sgn) {
     ps.in.so = ps.out.so = M;
     ps.in.sk = ps.out.sk = 1;
     ps.fast_io = true;
-    ps.variant = VARIANT_DIRECT;
-    Pass fp;
-    try {
-      fp = make_pass(ps);
-    } catch (const Error&) {
-      ps.variant = VARIANT_DYNAMIC;
-      fp = make_pass(ps);
+    std::vector<Pass> fp;
+    const size_t sb = add_direct_passes(fp, ps, 0, BUF_IN, BUF_OUT);
+    if (sb) cuda_check(cudaMalloc(&dS, sb), "cudaMalloc(bluestein filter scratch)");
+    for (const Pass& q : fp) {
+      void* bufs[4] = {dB, dB, nullptr, dS};
+      cuda_check(launch_pass(q, static_cast<char*>(bufs[q.src]) + q.src_off,
+                             static_cast<char*>(bufs[q.dst]) + q.dst_off, 0),
+                 "bluestein filter FFT");
     }
-    cuda_check(launch_pass(fp, dB, dB, 0), "bluestein filter FFT");
     cuda_check(cudaMemcpy(F.data(), dB, F.size() * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
   } catch (...) {
     cudaFree(dB);
+    if (dS) cudaFree(dS);
     throw;
   }
   cudaFree(dB);
+  if (dS) cudaFree(dS);
   std::vector<long double> br(M), bi(M);
   for (int k = 0; k < M; ++k) {
     br[k] = (long double)F[2 * k] / M;
@@ -1212,7 +1360,11 @@ size_t add_axis_passes(std::vector<Pass>& out, const PassSpec& s, unsigned flags
     if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
   }
   const int L = s.L;
-  if (L > (1 << 20)) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "length too large for Bluestein"};
+  if (plain_complex_axis(s)) {
+    int L1 = 0, L2 = 0;
+    if (four_step_split(s.dbl, L, &L1, &L2)) return add_four_step(out, s, L1, L2, src, dst);
+  }
+  if (L > (1 << 23)) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "length too large for Bluestein"};
   // the outer direction is in the tables; the inner FFT_M pair is forward
   // then inverse
   BluesteinTables bt = bluestein_tables(s.dbl, L, s.inverse ? +1 : -1);
@@ -1251,15 +1403,43 @@ size_t add_axis_passes(std::vector<Pass>& out, const PassSpec& s, unsigned flags
   b.out.chirp_n = L;
   b.keep.push_back(bt.chirp);
   b.keep.push_back(bt.bhat);
-  Pass pa = make_pass(a);
+  const size_t scratch = (size_t)(s.I * s.O) * (size_t)M * csz;
+  Pass pa, pb;
+  try {
+    pa = make_pass(a);
+    pb = make_pass(b);
+  } catch (const Error& e) {
+    if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
+    // FFT_M does not fit one CTA: each FFT_M as a four-step pair, through
+    // two scratch halves: x * chirp -> S1 -> S2 (the spectrum),
+    // S2 * Bhat -> S1 -> out * chirp.  The last pass's sub-axis index
+    // k2 < M2 must stay below L (its column bases lie in the output).
+    int M1 = 0, M2 = 0;
+    if (!plain_complex_axis(s) || !four_step_split(s.dbl, M, &M1, &M2) || M2 > L)
+      throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "length " + std::to_string(L) + " is too long for Bluestein here"};
+    Pass p[4];
+    four_step_pair(a, M1, M2, &p[0], &p[1]);
+    four_step_pair(b, M1, M2, &p[2], &p[3]);
+    p[0].src = src;
+    p[0].dst = BUF_CHIRP;
+    p[1].src = BUF_CHIRP;
+    p[1].dst = BUF_CHIRP;
+    p[1].dst_off = scratch;
+    p[2].src = BUF_CHIRP;
+    p[2].src_off = scratch;
+    p[2].dst = BUF_CHIRP;
+    p[3].src = BUF_CHIRP;
+    p[3].dst = dst;
+    for (Pass& q : p) out.push_back(std::move(q));
+    return 2 * scratch;
+  }
   pa.src = src;
   pa.dst = BUF_CHIRP;
-  Pass pb = make_pass(b);
   pb.src = BUF_CHIRP;
   pb.dst = dst;
   out.push_back(std::move(pa));
   out.push_back(std::move(pb));
-  return (size_t)(s.I * s.O) * (size_t)M * csz;
+  return scratch;
 }
 
 }  // namespace dfft

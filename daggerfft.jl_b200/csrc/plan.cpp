@@ -350,7 +350,8 @@ void execute_plan(const Plan* P, const void* in, void* out, cudaStream_t stream,
   for (const Pass& p : P->passes) {
     if (err != cudaSuccess) break;
     void* bufs[4] = {const_cast<void*>(in), out, work, chirp};
-    err = launch_pass(p, bufs[p.src], bufs[p.dst], stream, work);
+    err = launch_pass(p, static_cast<char*>(bufs[p.src]) + p.src_off, static_cast<char*>(bufs[p.dst]) + p.dst_off,
+                      stream, work);
   }
   if (cur != P->device) cudaSetDevice(cur);
   cuda_check(err, "kernel launch");

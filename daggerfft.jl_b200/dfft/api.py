@@ -408,14 +408,16 @@ def ifft_(A, decomp=None, dims=(1, 2, 3), method="plain"):
 
 
 class Batch:
-    """Independent plans executed together (``dfft_batch_*``): one launch of
+    """Independent plans executed together (``dfft_batch_*``): one CUDA
+    graph of the plans' passes, or, with ``persistent=True``, one launch of
     the persistent batch kernel when every plan is a complex transform of
-    the lengths it runs (``launches == 1``), otherwise one CUDA graph of the
-    plans' passes (``graph=True`` forces the graph).  ``execute(ins, outs)``
-    takes one input and one output tensor per plan; a graph is captured on
-    the first call and replayed while the same buffers are passed."""
+    the lengths it runs (``launches == 1``; ``lag`` staggers a pass behind
+    its predecessor in the work list, 0 = automatic).  ``execute(ins,
+    outs)`` takes one input and one output tensor per plan; a graph is
+    captured on the first call and replayed while the same buffers are
+    passed."""
 
-    def __init__(self, plans: Sequence[Plan], graph: bool = False):
+    def __init__(self, plans: Sequence[Plan], persistent: bool = False, lag: int = 0):
         L = _lib.lib()
         self._L = L
         self.plans = list(plans)  # keeps the plans alive
@@ -431,7 +433,10 @@ class Batch:
         L.dfft_batch_destroy.restype = ctypes.c_int
         arr = (ctypes.c_void_p * len(self.plans))(*[p._h.value for p in self.plans])
         h = ctypes.c_void_p()
-        check(L.dfft_batch_create_ex(ctypes.byref(h), len(self.plans), arr, 1 if graph else 0))
+        if not 0 <= lag <= 255:
+            raise ArgumentError(_lib.ERROR_INVALID_VALUE, "lag must be in 0..255")
+        flags = (2 if persistent else 0) | (lag << 8)
+        check(L.dfft_batch_create_ex(ctypes.byref(h), len(self.plans), arr, flags))
         self._h = h
         n = ctypes.c_int()
         check(L.dfft_batch_launches(h, ctypes.byref(n)))

@@ -177,15 +177,20 @@ function device_error()
     Int(c[])
 end
 
-# ---- batches of uneven transforms (one CUDA graph launch) -------------------
+# ---- batches of uneven transforms (one CUDA graph launch, or one launch of
+# the persistent batch kernel with `persistent = true`) ----------------------
+const BATCH_PERSISTENT = Cuint(1) << 1
+
 mutable struct Batch
     h::Ptr{Cvoid}
     plans::Vector{Plan}   # kept alive as long as the batch
-    function Batch(plans::Vector{Plan})
+    function Batch(plans::Vector{Plan}; persistent::Bool = false, lag::Integer = 0)
+        0 <= lag <= 255 || throw(ArgumentError("lag must be in 0..255"))
         h = Ref{Ptr{Cvoid}}(C_NULL)
         hs = Ptr{Cvoid}[p.h for p in plans]
-        check(ccall((:dfft_batch_create, libdfft), Cint, (Ptr{Ptr{Cvoid}}, Cint, Ptr{Ptr{Cvoid}}),
-                    h, length(hs), hs))
+        flags = (persistent ? BATCH_PERSISTENT : Cuint(0)) | (Cuint(lag) << 8)
+        check(ccall((:dfft_batch_create_ex, libdfft), Cint,
+                    (Ptr{Ptr{Cvoid}}, Cint, Ptr{Ptr{Cvoid}}, Cuint), h, length(hs), hs, flags))
         b = new(h[], plans)
         finalizer(b) do q
             q.h != C_NULL && ccall((:dfft_batch_destroy, libdfft), Cint, (Ptr{Cvoid},), q.h)

@@ -171,22 +171,30 @@ DFFT_API int dfft_wisdom_size(int* n);
 /* ---- batches of uneven transforms -----------------------------------
  *
  * No counterpart in the reference (north-star addition): N independent
- * plans (any shapes/kinds) executed together.  When every plan is a complex
- * transform (FFT / IFFT, one precision) whose axis lengths the persistent
- * batch kernel runs (16, 24, 32, 40, 48, 60, 64, 72, 80, 96, 100, 120, 128,
- * 144, 160, 192, 256), the batch is ONE kernel launch over a work list of
- * every axis pass of every transform (passes of one transform run in its
- * stage order; a pass waits, bounded, for its predecessor).  Otherwise the
- * first execute with a set of buffers captures every plan's passes as
- * concurrent branches of a CUDA graph; later executes with the same buffers
- * replay the graph, new buffers update it.  Plans must outlive the batch and
- * live on the current device.  dfft_batch_launches reports which: 1 for the
- * persistent kernel, else the graph's kernel count.
+ * plans (any shapes/kinds) executed together.  By default the first execute
+ * with a set of buffers captures every plan's passes as concurrent branches
+ * of a CUDA graph (the branch count keeps the transforms in flight within
+ * L2); later executes with the same buffers replay the graph, new buffers
+ * update it.  With DFFT_BATCH_PERSISTENT, a batch whose plans are all
+ * complex transforms (FFT / IFFT, one precision) of axis lengths the
+ * persistent batch kernel runs (16, 24, 32, 40, 48, 60, 64, 72, 80, 96,
+ * 100, 120, 128, 144, 160, 192, 256) is instead ONE kernel launch over a
+ * work list of every axis pass of every transform (a pass waits, bounded,
+ * for its predecessor; bits 8-15 of the flags give the stagger `lag`
+ * between a pass and its predecessor in the list, 0 = automatic); other
+ * batches keep the graph.  The graph is the faster form on B200 for the
+ * shapes measured here; the persistent form is kept for callers that need
+ * a single launch.  Plans must outlive the batch and live on the current
+ * device.  dfft_batch_launches reports which: 1 for the persistent kernel,
+ * else the graph's kernel count.
  */
 typedef struct dfft_batch_s* dfft_batch;
-enum { DFFT_BATCH_GRAPH = 1u << 0 /* always the graph of the plans' own passes */ };
+enum {
+  DFFT_BATCH_GRAPH = 1u << 0,      /* the graph of the plans' own passes (the default) */
+  DFFT_BATCH_PERSISTENT = 1u << 1  /* one persistent-kernel launch where eligible */
+};
 DFFT_API int dfft_batch_create(dfft_batch* batch, int nplans, const dfft_plan* plans);
-/* The same with flags (DFFT_BATCH_GRAPH). */
+/* The same with flags (DFFT_BATCH_GRAPH / DFFT_BATCH_PERSISTENT | lag << 8). */
 DFFT_API int dfft_batch_create_ex(dfft_batch* batch, int nplans, const dfft_plan* plans, unsigned flags);
 DFFT_API int dfft_batch_execute(dfft_batch batch, const void* const* ins, void* const* outs,
                                 void* stream);

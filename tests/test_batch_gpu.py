@@ -1,4 +1,5 @@
-"""Batches of uneven transforms in one graph launch (configuration: 64
+"""Batches of uneven transforms in one graph launch (or one persistent-kernel
+launch on request) (configuration: 64
 independent 3-D C2C ComplexF32 grids with edges from
 {48,64,80,96,120,128,160,192}, plus a 2-D DCT-II/III Float64 stack), each
 result checked against the oracle and against the same plan run alone."""
@@ -20,18 +21,18 @@ def _grids(n, seed=0):
     return [tuple(int(e) for e in rng.choice(EDGES, 3)) for _ in range(n)]
 
 
-@pytest.mark.parametrize("graph", [False, True])
-def test_batch_uneven_grids_match_oracle_and_alone(graph):
-    # graph=False: one launch of the persistent batch kernel (these lengths
-    # are all in its set); graph=True: the graph of the plans' own passes,
-    # bit-identical to each plan run alone
+@pytest.mark.parametrize("persistent", [False, True])
+def test_batch_uneven_grids_match_oracle_and_alone(persistent):
+    # default: the graph of the plans' own passes, bit-identical to each plan
+    # run alone; persistent=True: one launch of the persistent batch kernel
+    # (these lengths are all in its set), equal to rounding
     shapes = _grids(12, seed=1)
     arrays = [rand(s, np.complex64, seed=i, kind="uniform11") for i, s in enumerate(shapes)]
     ins = [to_gpu(a) for a in arrays]
     plans = [dfft.gpu_plan_transform(dfft.FFT(), g, (1, 2, 3), flags=dfft.FLAG_TUNE) for g in ins]
     outs = [dfft.empty_like_layout(p.out_shape, g.dtype, g) for p, g in zip(plans, ins)]
-    b = dfft.Batch(plans, graph=graph)
-    assert b.launches == (sum(p.launches for p in plans) if graph else 1)
+    b = dfft.Batch(plans, persistent=persistent)
+    assert b.launches == (1 if persistent else sum(p.launches for p in plans))
     for rep in range(3):  # capture, then replays of the same graph
         b.execute(ins, outs)
         torch.cuda.synchronize()
@@ -39,7 +40,7 @@ def test_batch_uneven_grids_match_oracle_and_alone(graph):
             assert rel(to_np(o), oracle.fft(a, dims=(1, 2, 3))) <= 1e-5
             alone = dfft.empty_like_layout(p.out_shape, g.dtype, g)
             p.execute(g, alone)
-            if graph:
+            if not persistent:
                 assert torch.equal(alone, o), "batched result differs from the plan run alone"
             else:  # other kernels than the plan's: equal to rounding
                 assert rel(to_np(o), to_np(alone)) <= 1e-6
@@ -68,7 +69,8 @@ def test_batch_mixes_kinds_and_precisions():
     assert rel(to_np(outs[2]), oracle.fft(d, dims=(1, 2), transforms=(oracle.R2R((oracle.REDFT10, oracle.REDFT10)),))) <= 1e-12
 
 
-def test_persistent_batch_inverse_and_float64():
+@pytest.mark.parametrize("lag", [0, 1, 3])
+def test_persistent_batch_inverse_and_float64(lag):
     # inverse transforms (reverse stage order, 1/N) and ComplexF64, 2-D and 3-D
     shapes = [(48, 64, 40), (96, 24), (160, 120, 16), (32, 256, 16)]
     for dt, tol in ((np.complex64, 1e-5), (np.complex128, 1e-12)):
@@ -76,7 +78,7 @@ def test_persistent_batch_inverse_and_float64():
         ins = [to_gpu(a) for a in arrays]
         plans = [dfft.gpu_plan_transform(dfft.IFFT(), g, tuple(range(1, g.dim() + 1))) for g in ins]
         outs = [dfft.empty_like_layout(p.out_shape, g.dtype, g) for p, g in zip(plans, ins)]
-        b = dfft.Batch(plans)
+        b = dfft.Batch(plans, persistent=True, lag=lag)
         assert b.launches == 1
         for _ in range(2):
             b.execute(ins, outs)
@@ -91,7 +93,7 @@ def test_persistent_batch_falls_back_to_graph():
     a = rand((77, 32, 8), np.complex64, seed=1)
     g = to_gpu(a)
     p = dfft.gpu_plan_transform(dfft.FFT(), g, (1, 2, 3))
-    b = dfft.Batch([p])
+    b = dfft.Batch([p], persistent=True)
     assert b.launches == p.launches
     o = dfft.empty_like_layout(p.out_shape, g.dtype, g)
     b.execute([g], [o])

@@ -127,9 +127,10 @@ def test_unknown_transform_and_bad_args():
         dfft.get_or_create_gpu_plan("not a tag", g, (1,))
     with pytest.raises(dfft.ArgumentError):
         dfft.fft(g, dims=(3,))
-    # a prime length beyond what one CTA can convolve is rejected, not faked
+    # a prime length beyond the longest Bluestein convolution (2^23) is
+    # rejected, not faked
     with pytest.raises(dfft.ArgumentError):
-        dfft.fft(torch.zeros((32771,), dtype=torch.complex64, device="cuda"), dims=(1,))
+        dfft.fft(torch.zeros((8388617,), dtype=torch.complex64, device="cuda"), dims=(1,))
 
 
 @pytest.mark.parametrize("shape", [(512, 64, 48), (64, 512, 8), (96, 96, 96), (256, 8, 512)])

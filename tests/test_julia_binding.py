@@ -145,7 +145,7 @@ def test_every_ccall_matches_the_header():
 def test_binding_covers_the_entry_points_a_julia_user_needs():
     names = {n for n, _, _ in julia_ccalls()}
     need = {"dfft_plan_create", "dfft_execute", "dfft_plan_destroy", "dfft_plan_output_shape",
-            "dfft_plan_describe", "dfft_wisdom_export", "dfft_wisdom_import", "dfft_batch_create",
+            "dfft_plan_describe", "dfft_wisdom_export", "dfft_wisdom_import", "dfft_batch_create_ex",
             "dfft_batch_execute", "dfft_server_create", "dfft_server_submit", "dfft_server_wait",
             "dfft_server_poll", "dfft_server_get_stats", "dfft_server_release", "dfft_copy_plan_create",
             "dfft_copy_plan_execute", "dfft_last_error"}

@@ -1,0 +1,98 @@
+"""Complex axes longer than one CTA holds run as a four-step pair of passes
+(L = L1 * L2: L2-point transforms, the twiddle W_L^(n1 k2) on the way out,
+then L1-point transforms written to k2 + L2 k1) instead of Bluestein's
+passes of length >= 2L; prime axes whose Bluestein length M exceeds one CTA
+run that convolution as two four-step pairs.  Checked against the FP64
+oracle at the precision's stated tolerance, forward and inverse, on
+contiguous and strided axes, for static and dynamic factors."""
+import numpy as np
+import pytest
+import torch
+
+import dfft
+import dfft_oracle as oracle
+from helpers import rand, rel, to_gpu, to_np, tol_for
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(transform, g, dims):
+    p = dfft.gpu_plan_transform(transform, g, dims)
+    out = dfft.empty_like_layout(p.out_shape, g.dtype, g)
+    p.execute(g, out)
+    torch.cuda.synchronize()
+    return p, out
+
+
+def _four_step_lines(p):
+    return [ln for ln in p.describe().splitlines() if "four-step" in ln]
+
+
+@pytest.mark.parametrize("dtype,shape,dims", [
+    (np.complex64, (65536,), (1,)),            # 256 x 256
+    (np.complex64, (1 << 20,), (1,)),          # 1024 x 1024
+    (np.complex64, (196608, 2), (1,)),         # 384 x 512, two pencils
+    (np.complex64, (1000000,), (1,)),          # 1000 x 1000
+    (np.complex64, (4, 32768, 3), (2,)),       # strided long axis, I = 4
+    (np.complex64, (8, 65536, 5), (1, 2, 3)),  # long axis among short ones
+    (np.complex64, (64064,), (1,)),            # 7 * 11 * 13 * 64: dynamic factors
+    (np.complex128, (1 << 20,), (1,)),         # 1024 x 1024
+    (np.complex128, (3, 40000, 2), (2,)),      # strided, 200 x 200
+    (np.complex128, (200704,), (1,)),          # 392 (dynamic) x 512 (static)
+])
+def test_long_axis_matches_oracle(dtype, shape, dims):
+    a = rand(shape, dtype, seed=len(shape) + shape[0] % 97)
+    g = to_gpu(a)
+    p, F = _run(dfft.FFT(), g, dims)
+    assert len(_four_step_lines(p)) >= 2, p.describe()
+    tol = tol_for(dtype)
+    assert rel(to_np(F), oracle.fft(a, dims=dims)) <= tol
+    _, B = _run(dfft.IFFT(), F, dims)
+    assert rel(to_np(B), oracle.ifft(to_np(F), dims=dims)) <= tol
+    assert rel(to_np(B), a) <= tol
+    assert dfft.device_error() == 0
+
+
+def test_long_axis_impulse_and_constant():
+    # exact spectra: an impulse at n0 gives W^(n0 k), a constant gives L at k = 0
+    L = 1 << 16
+    a = np.zeros(L, np.complex128)
+    a[12345] = 1
+    _, F = _run(dfft.FFT(), to_gpu(a), (1,))
+    k = np.arange(L)
+    # the phase reduced exactly modulo L (2 pi * 12345 * k / L itself would
+    # carry ~1e-11 of FP64 rounding)
+    assert np.max(np.abs(to_np(F) - np.exp(-2j * np.pi * ((12345 * k) % L) / L))) <= 1e-12
+    c = np.ones(L, np.complex128)
+    _, F = _run(dfft.FFT(), to_gpu(c), (1,))
+    Fh = to_np(F)
+    assert abs(Fh[0] - L) <= 1e-9 and np.max(np.abs(Fh[1:])) <= 1e-9
+
+
+def test_long_axis_in_place():
+    a = rand((1 << 18,), np.complex64, seed=3)
+    g = to_gpu(a)
+    p = dfft.gpu_plan_transform(dfft.FFT(), g, (1,))
+    p.execute(g, g)
+    torch.cuda.synchronize()
+    assert rel(to_np(g), oracle.fft(a, dims=(1,))) <= 1e-5
+
+
+@pytest.mark.parametrize("dtype,shape,dims", [
+    (np.complex64, (32771,), (1,)),        # M = 65610 = 243 x 270
+    (np.complex64, (65537, 2), (1,)),      # M = 131220, two pencils
+    (np.complex128, (3, 100003), (2,)),    # strided, M = 202500
+    (np.complex64, (1000003,), (1,)),      # M = 2025000
+])
+def test_prime_long_axis_bluestein_over_four_step(dtype, shape, dims):
+    # a long prime axis: Bluestein's length-M convolution runs as two
+    # four-step pairs (chirp on the first load, the filter on the third
+    # pass's load, chirp and truncation on the last store)
+    a = rand(shape, dtype, seed=shape[0] % 101)
+    p, F = _run(dfft.FFT(), to_gpu(a), dims)
+    assert len(_four_step_lines(p)) == 4, p.describe()
+    tol = tol_for(dtype)
+    assert rel(to_np(F), oracle.fft(a, dims=dims)) <= tol
+    _, B = _run(dfft.IFFT(), F, dims)
+    assert rel(to_np(B), a) <= tol
+    assert dfft.device_error() == 0
