@@ -109,6 +109,11 @@ const TiledKernel* find_tiled_kernel(int dbl, int L, int strided, int kind);
 // (scales: 1 forward, 1/L per axis inverse) with launch variant v; throws
 // Error{DFFT_ERROR_UNSUPPORTED_SIZE} when that variant cannot serve the shape.
 Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v = 0);
+// The same pass over nslab slabs with rank-split input (rin rows per rank)
+// and/or output (rout rows per rank), zr slabs between one rank's blocks
+// (SlabGeom); rin = rout = L is make_slab_pass.
+Pass make_slab_split_pass(int dbl, int L, long long nslab, int inverse, int v, int rin, int rout,
+                          long long zr);
 
 // Fused variant to use for dims (1, 2) of an L x L x O array, or -1 for the
 // per-axis passes `split` (x then y, already planned): wisdom, then timing

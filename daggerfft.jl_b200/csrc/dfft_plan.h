@@ -31,6 +31,11 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
                  const int32_t* dims, const int32_t* r2r_kinds, int64_t irfft_len, int decomp,
                  int method, unsigned flags);
 
+// The fused 2-D slab pass of a distributed Slab transform with the output
+// (forward) or input (inverse) in the rank-split layout (dfft_slab_split_create).
+Plan* build_slab_split_plan(int precision, int inverse, int64_t L, int64_t nslab, int64_t zr, int nranks,
+                            unsigned flags);
+
 // work / chirp: workspaces supplied by the caller for this execution (null:
 // the plan's own); a plan built with kFlagCallerWorkspace owns none.
 void execute_plan(const Plan* p, const void* in, void* out, cudaStream_t stream, void* work = nullptr,

@@ -934,6 +934,8 @@ Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v) {
   p.d2.tw2 = twl->p;
   SlabGeom& g = p.sgeom;
   g.nslab = O;
+  g.rin = g.rout = L;
+  g.zr = O;
   g.tiles = L / k->cs;
   g.xscale = dbl ? 2 : 1;
   g.lb = box_rows(L);
@@ -972,6 +974,35 @@ Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v) {
   // x-jobs by more rounds than the jobs in flight span
   g.lag = (int)((nb * (k->nb + kSlabClaim) + 2LL * g.tiles - 1) / (2LL * g.tiles)) + 1;
   p.ctr_bytes = 8 + 4 * (size_t)O;
+  return p;
+}
+
+Pass make_slab_split_pass(int dbl, int L, long long nslab, int inverse, int v, int rin, int rout,
+                          long long zr) {
+  Pass p = make_slab_pass(dbl, L, nslab, inverse, v);
+  SlabGeom& g = p.sgeom;
+  const int cs = p.geom.C;
+  auto ok_rows = [&](int R) { return R >= 1 && R <= L && L % R == 0; };
+  if (!ok_rows(rin) || !ok_rows(rout) || zr < nslab)
+    throw Error{DFFT_ERROR_INVALID_VALUE, "rank split: rows per rank must divide L, zr >= slabs"};
+  // a tile's pencils stay contiguous, and no TMA box straddles two ranks'
+  // rows (boxes of the largest divisor of rout up to the plain box height)
+  if (rin % cs != 0 || rout % cs != 0)
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "rank split: rows per rank do not hold whole tiles"};
+  while (rout % g.lb != 0) --g.lb;
+  g.nlb = L / g.lb;
+  p.geom.lb = g.lb;
+  const size_t esz = dbl ? 16 : 8;
+  if (g.nlb > 1 && ((size_t)g.lb * cs * esz) % 128 != 0)
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "rank split: TMA box offsets would not be 128-byte aligned"};
+  const long long zmax = zr * (long long)(L / rout - 1) + nslab;  // slab coordinates the map spans
+  const long long zin = zr * (long long)(L / rin - 1) + nslab;
+  if (zmax >= (1LL << 31) || zin >= (1LL << 31)) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "rank split too large"};
+  g.rin = rin;
+  g.rout = rout;
+  g.zr = zr;
+  p.tL = rout;
+  p.tO = zmax;
   return p;
 }
 

@@ -320,6 +320,54 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
   return P.release();
 }
 
+Plan* build_slab_split_plan(int precision, int inverse, int64_t L, int64_t nslab, int64_t zr, int nranks,
+                            unsigned flags) {
+  if (precision != DFFT_F32 && precision != DFFT_F64)
+    throw Error{DFFT_ERROR_INVALID_VALUE, "precision must be DFFT_F32 or DFFT_F64"};
+  if (L < 1 || L > 0x7fffffffLL || nslab < 1 || zr < nslab || nranks < 1 || L % nranks != 0)
+    throw Error{DFFT_ERROR_INVALID_VALUE, "slab split: need L % nranks == 0, 1 <= nslab <= zr"};
+  const int dbl = precision == DFFT_F64 ? 1 : 0;
+  const int64_t R = L / nranks;
+  std::unique_ptr<Plan> P(new Plan());
+  P->ndim = 3;
+  P->precision = precision;
+  P->transform = inverse ? DFFT_IFFT : DFFT_FFT;
+  P->decomp = DFFT_SLAB;
+  P->method = DFFT_PLAIN;
+  P->flags = flags;
+  P->dims = {0, 1};
+  cuda_check(cudaGetDevice(&P->device), "cudaGetDevice");
+  P->in_elem = P->out_elem = dbl ? 16 : 8;
+  const int64_t plain[3] = {L, L, nslab};
+  const int64_t split[3] = {L, R, zr * (nranks - 1) + nslab};  // the span of the rank blocks
+  for (int i = 0; i < 3; ++i) {
+    P->in_shape[i] = inverse ? split[i] : plain[i];
+    P->out_shape[i] = inverse ? plain[i] : split[i];
+  }
+  const int rin = (int)(inverse ? R : L), rout = (int)(inverse ? L : R);
+  bool made = false;
+  std::string why = "no fused slab kernel for this length";
+  for (int v = 0; const SlabKernel* k = find_slab_kernel(dbl, (int)L, v); ++v) {
+    if (!k->dflt) continue;
+    try {
+      Pass p = make_slab_split_pass(dbl, (int)L, nslab, inverse, v, rin, rout, zr);
+      p.src = BUF_IN;
+      p.dst = BUF_OUT;
+      P->work_bytes = p.ctr_bytes;
+      P->passes.push_back(std::move(p));
+      made = true;
+      break;
+    } catch (const Error& e) {
+      if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
+      why = e.msg;
+    }
+  }
+  if (!made) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "slab split: " + why};
+  if (!(flags & kFlagCallerWorkspace))
+    cuda_check(cudaMalloc(&P->work, P->work_bytes), "cudaMalloc(workspace)");
+  return P.release();
+}
+
 Plan::~Plan() {
   if (work || chirp) {
     int cur = -1;

@@ -48,6 +48,15 @@ struct SlabGeom {
   int lb, nlb;       // rows per TMA box, boxes per y tile
   int ntw;           // stage-twiddle entries staged in shared memory
   int bstride;       // elements between tile buffers (128-byte multiple)
+  // Rank-split layouts (distributed Slab exchange).  A side with R rows per
+  // rank holds row y of slab z (a pencil of L elements) at row
+  //   (y mod R) + R * (z + zr * (y / R)),
+  // so the rows every rank owns (R of them per slab) form one contiguous
+  // block per rank.  R = L is the plain layout.  The x-phase reads the
+  // input with rin and writes the output with rout; the y-phase reads and
+  // writes the output (tensor map {L, rout, ...}) with rout.
+  int rin, rout;
+  long long zr;
   unsigned long long* jobs;  // next job in the sequence
   unsigned* done;            // x-tiles finished, per slab
   int* err;
@@ -120,6 +129,12 @@ template <typename V, int CS, int R0> struct YSwzCol {
 };
 template <int R, int... Rest> struct first_radix { static constexpr int value = R; };
 
+// Row index (in units of L elements) of row y of slab z in a side with R
+// rows per rank (see SlabGeom).
+__device__ __forceinline__ long long split_row(int R, long long zr, long long z, int y) {
+  return (long long)(y % R) + (long long)R * (z + zr * (long long)(y / R));
+}
+
 // dx: x-phase descriptor (in -> out, contiguous pencils, FAST_IO global
 // stores); dy: y-phase descriptor (scale / inverse of the second axis).
 // tout: tensor map {L*xscale, L, O} over the output (y-phase loads/stores).
@@ -186,8 +201,11 @@ __global__ void __launch_bounds__(LB, MINB)
           asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(g.done + slabb[b]) : "memory");
         } else {
           const V* buf = bufs + b * bst;
-          for (int kb = 0; kb < g.nlb; ++kb)
-            tma_store_3d(&tout, buf + (size_t)kb * g.lb * CS, tileb[b] * CS * g.xscale, kb * g.lb, slabb[b]);
+          for (int kb = 0; kb < g.nlb; ++kb) {
+            const int y = kb * g.lb;  // boxes never straddle a rank's rows (lb divides rout)
+            tma_store_3d(&tout, buf + (size_t)kb * g.lb * CS, tileb[b] * CS * g.xscale, y % g.rout,
+                         (int)(slabb[b] + g.zr * (y / g.rout)));
+          }
           bulk_commit();
           bulk_wait_read_all();
         }
@@ -246,12 +264,16 @@ __global__ void __launch_bounds__(LB, MINB)
         V* buf = bufs + b * bst;
         mbar_expect_tx(&full[b], tile_bytes);
         if (J.kind == 1) {
-          bulk_load_1d(buf, reinterpret_cast<const V*>(dx.in.p) + ((long long)J.slab * L + (long long)J.tile * CS) * L,
+          // CS divides rin: the tile's CS pencils are contiguous in both layouts
+          bulk_load_1d(buf, reinterpret_cast<const V*>(dx.in.p) + split_row(g.rin, g.zr, J.slab, J.tile * CS) * L,
                        tile_bytes, &full[b]);
         } else {
           fence_proxy_async_global();  // x-phase writes (generic proxy) before these async-proxy reads
-          for (int kb = 0; kb < g.nlb; ++kb)
-            tma_load_3d(buf + (size_t)kb * g.lb * CS, &tout, &full[b], J.tile * CS * g.xscale, kb * g.lb, J.slab);
+          for (int kb = 0; kb < g.nlb; ++kb) {
+            const int y = kb * g.lb;
+            tma_load_3d(buf + (size_t)kb * g.lb * CS, &tout, &full[b], J.tile * CS * g.xscale, y % g.rout,
+                        (int)(J.slab + g.zr * (y / g.rout)));
+          }
         }
         kindb[b] = J.kind;
         slabb[b] = J.slab;
@@ -287,7 +309,7 @@ __global__ void __launch_bounds__(LB, MINB)
         const int t = tid % P, c = tid / P;
         const StrideCol<V> dense{buf + (size_t)c * L, 1};
         const XSwzCol<V, L, R0> sw{buf + (size_t)c * L, c};
-        const long long ob = ((long long)J.slab * L + (long long)J.tile * CS + c) * L;
+        const long long ob = split_row(g.rout, g.zr, J.slab, J.tile * CS + c) * L;
         static_stages<T, L, P, true, 2, NC, DIR, 1, 1, 0, StrideCol<V>, XSwzCol<V, L, R0>, XSwzCol<V, L, R0>,
                       TWT, Rs...>(dx, t, dense, sw, sw, tw, 0, ob, true);
         fence_proxy_async_global();  // these stores are read by bulk-tensor loads

@@ -18,5 +18,6 @@ from .darray import (Blocks, CudaCopier, DArray, Workspace, collect, compute_ove
                      gpu_coalesced_redistribute_, gpu_fft_, gpu_ifft_)
 
 from .serve import Server
+from .slab_dist import FusedSlabFFT, SlabSplitPlan
 
 __version__ = "0.1.0"

@@ -374,6 +374,48 @@ def _inplace(t):
     raise ArgumentError(_lib.ERROR_UNKNOWN_TRANSFORM, "Unknown transform type")
 
 
+def _fused_slab(ws: Workspace, Az: DArray, By: DArray, transforms, dims, group, inverse):
+    """The fused Slab exchange (dfft.slab_dist) for this pair of layouts, or
+    None: L x L x N3 complex chunks on CUDA, one z-block per rank in A
+    (Blocks(L, L, ceil(N3 / P))), one y-block per rank in B
+    (Blocks(L, L / P, N3)), dims (1, 2, 3), FFT / IFFT tags."""
+    fam = (IFFT, IFFT_) if inverse else (FFT, FFT_)
+    if tuple(dims) != (1, 2, 3) or not all(isinstance(t, fam) for t in transforms):
+        return None
+    if Az.dtype not in (torch.complex64, torch.complex128):
+        return None
+    n1, n2, n3 = Az.shape
+    if n1 != n2 or tuple(By.shape) != tuple(Az.shape):
+        return None
+    world, rank = 1, Az.rank
+    try:
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            world = dist.get_world_size(group)
+    except Exception:
+        return None
+    if n1 % world or tuple(Az.blocks.b) != (n1, n2, -(-n3 // world)) or \
+            tuple(By.blocks.b) != (n1, n1 // world, n3):
+        return None
+    chunks = [c for c in Az.chunks if c is not None] + [c for c in By.chunks if c is not None]
+    if not chunks or not all(c.is_cuda for c in chunks):
+        return None
+    key = ("fused_slab", n1, n3, Az.dtype, world, rank)
+    cached = getattr(ws, "_fused", None)
+    if cached is not None and cached[0] == key:
+        return cached[1]
+    from .slab_dist import FusedSlabFFT, SlabSplitPlan
+    try:
+        # every rank (one without slabs too) builds a split plan now, so an
+        # unsupported length falls back on all ranks before any exchange
+        SlabSplitPlan(n1, 1, 1, world, Az.dtype, inverse, chunks[0].device)
+        fs = FusedSlabFFT(n1, n3, Az.dtype, rank, world, group=group, device=chunks[0].device)
+    except ArgumentError:
+        return None
+    ws._fused = (key, fs)
+    return fs
+
+
 def gpu_fft_(*args, group=None, stage=None, copier=None):
     """Pencil: ``gpu_fft!(C, A, B, wsAB, wsBC, transforms, dims, Pencil())``
     (src/fftgpu.jl:498-531); Slab: ``gpu_fft!(B, A, wsAB, transforms, dims,
@@ -387,6 +429,13 @@ def gpu_fft_(*args, group=None, stage=None, copier=None):
     decomp = args[-1]
     if isinstance(decomp, Slab):
         B, A, wsAB, transforms, dims, _ = args
+        fs = _fused_slab(wsAB, A, B, transforms, dims, group, False) if stage is None and copier is None else None
+        if fs is not None:
+            ia, ib = A.local_indices, B.local_indices
+            a = A.chunks[ia[0]] if ia else torch.empty((A.shape[0], A.shape[1], 0), dtype=A.dtype,
+                                                        device=B.chunks[ib[0]].device)
+            fs.forward(a, B.chunks[ib[0]])
+            return B
         st(A, _inplace(transforms[0]), (dims[0], dims[1]))
         gpu_coalesced_redistribute_(B, A, wsAB, 1, group, copier)
         st(B, _inplace(transforms[2]), (dims[2],))
@@ -411,6 +460,13 @@ def gpu_ifft_(*args, group=None, stage=None, copier=None):
     decomp = args[-1]
     if isinstance(decomp, Slab):
         A, B, wsBA, transforms, dims, _ = args
+        fs = _fused_slab(wsBA, A, B, transforms, dims, group, True) if stage is None and copier is None else None
+        if fs is not None:
+            ia, ib = A.local_indices, B.local_indices
+            a = A.chunks[ia[0]] if ia else torch.empty((A.shape[0], A.shape[1], 0), dtype=A.dtype,
+                                                        device=B.chunks[ib[0]].device)
+            fs.inverse(B.chunks[ib[0]], a)
+            return A
         st(B, _inplace(transforms[2]), (dims[2],))
         gpu_coalesced_redistribute_(A, B, wsBA, 3, group, copier)
         st(A, _inplace(transforms[0]), (dims[0], dims[1]))

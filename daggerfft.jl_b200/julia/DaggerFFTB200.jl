@@ -107,6 +107,36 @@ function execute!(p::Plan, out::CuArray, in::CuArray)
     out
 end
 
+"""
+    slab_split_plan(T, L, nslab, zr, nranks; inverse=false)
+
+The fused 2-D slab pass of a distributed Slab transform with the pack and
+unpack of the exchange folded in (`dfft_slab_split_create`): forward writes
+each rank's rows of every local slab as one contiguous block (the message
+to that rank), inverse reads the received blocks.  Run slab groups with
+`execute_split!` at element offsets; the blocks then go out with
+`MPI.Isend`/`MPI.Irecv!` and the received (L, L/P, N3) chunk takes a dims-3
+plan.
+"""
+function slab_split_plan(::Type{T}, L::Integer, nslab::Integer, zr::Integer, nranks::Integer;
+                         inverse::Bool=false) where {T}
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:dfft_slab_split_create, libdfft), Cint,
+                (Ptr{Ptr{Cvoid}}, Cint, Cint, Int64, Int64, Int64, Cint, Cuint),
+                h, precision_code(T), inverse ? Cint(1) : Cint(0), Int64(L), Int64(nslab), Int64(zr),
+                Cint(nranks), Cuint(0)))
+    out = zeros(Int64, 3)
+    check(ccall((:dfft_plan_output_shape, libdfft), Cint, (Ptr{Cvoid}, Ptr{Int64}), h[], out))
+    Plan(h[], Tuple(out))
+end
+
+"Run a split slab plan from `in` (element offset `ioff`) to `out` (offset `ooff`)."
+function execute_split!(p::Plan, out::CuArray{T}, ooff::Integer, in::CuArray{T}, ioff::Integer) where {T}
+    check(ccall((:dfft_execute, libdfft), Cint, (Ptr{Cvoid}, CuPtr{Cvoid}, CuPtr{Cvoid}, Ptr{Cvoid}),
+                p.h, pointer(in) + ioff * sizeof(T), pointer(out) + ooff * sizeof(T), CUDA.stream().handle))
+    out
+end
+
 "`apply_gpu_fft!(out, in, transform, dim)`: plan lookup + execute (src/fftgpu.jl:118-124)."
 function apply_gpu_fft!(out, in, transform, dim; kw...)
     execute!(plan_transform(transform, in, dim; kw...), out, in)
@@ -602,6 +632,7 @@ function gpu_cleanup_workspace!(ws::GPUWorkspace)
 end
 
 export fft, ifft, rfft, irfft, fft!, ifft!, apply_gpu_fft!, Pencil, Slab, R2R
+export slab_split_plan, execute_split!
 export Batch, launches, wisdom_export, wisdom_import, wisdom_forget, wisdom_size, device_error
 export Server, submit, poll, release, cancel, stats, reset_stats!, serve
 export ChunkedArray, distribute, distribute_empty, create_gpu_workspace, gpu_coalesced_redistribute!,

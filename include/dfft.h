@@ -118,6 +118,29 @@ DFFT_API int dfft_plan_create(dfft_plan* plan, int ndim, const int64_t* shape, i
                      int transform, int ndims, const int32_t* dims, const int32_t* r2r_kinds,
                      int64_t irfft_len, int decomp, int method, unsigned flags);
 
+/*
+ * Slab stage of a distributed Slab transform with the exchange's pack and
+ * unpack folded into it.  Replaces, for Slab with L % nranks == 0, the
+ * separate pack / unpack kernels around the exchange
+ * (src/fftgpu.jl:324-415 gpu_flat_redistribute!, :417-480 pack_kernel! /
+ * unpack_kernel!) next to the 2-D slab stage (src/fftgpu.jl:534-557 and
+ * :596-619).  The plan runs the fused dims-(1, 2) pass over `nslab` L x L
+ * slabs, one side in the RANK-SPLIT layout: with R = L / nranks rows per
+ * rank, row y of slab z (L contiguous elements) sits at row
+ *     (y mod R) + R * (z + zr * (y / R)),
+ * so rank s's rows of every slab form one contiguous block of zr * R * L
+ * elements (s = y / R).  Forward (inverse = 0): plain L x L x nslab input,
+ * split output -- block s is what this rank sends to rank s, and the
+ * blocks a rank receives, in sender order, are its (x, y in its rows, z)
+ * array for the last-axis pass.  Inverse (inverse = 1): split input (the
+ * received blocks), plain output.  zr >= nslab is the stride between rank
+ * blocks in slabs: running slab groups z0.. of one local array means
+ * offsetting the plain side by z0 * L * L and the split side by
+ * z0 * R * L elements with the same zr.  Execute with dfft_execute.
+ */
+DFFT_API int dfft_slab_split_create(dfft_plan* plan, int precision, int inverse, int64_t L, int64_t nslab,
+                                    int64_t zr, int nranks, unsigned flags);
+
 /* Output shape (column-major, ndim entries) of a plan. */
 DFFT_API int dfft_plan_output_shape(dfft_plan plan, int64_t* shape);
 
