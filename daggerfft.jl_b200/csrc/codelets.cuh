@@ -35,6 +35,36 @@ template <typename V> __device__ __forceinline__ V cmul(V a, V b) {
 }
 template <typename V> __device__ __forceinline__ V cconj(V a) { return mk<V>(a.x, -a.y); }
 template <typename V, typename S> __device__ __forceinline__ V cscale(V a, S s) { return mk<V>(a.x * s, a.y * s); }
+// ComplexF32 adds and subtracts as packed two-lane FP32 instructions
+// (add / sub.rn.f32x2, sm_100; the same round-to-nearest sums as the scalar
+// form).  Half the issue slots for the butterflies: the fused slab pass,
+// bound by instruction issue, runs 9 % faster with them (512^3, B200); the
+// 1024-thread strided pass, bound by its barriers, runs 15 % slower.  A
+// translation unit opts in by defining DFFT_PACKED_F32 before including
+// this header.
+#ifdef DFFT_PACKED_F32
+__device__ __forceinline__ unsigned long long f2bits(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ float2 bitsf2(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2bits(a)), "l"(f2bits(b)));
+  return bitsf2(r);
+}
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2bits(a)), "l"(f2bits(b)));
+  return bitsf2(r);
+}
+#endif
+
 // multiply by -i and +i
 template <typename V> __device__ __forceinline__ V cmul_mi(V a) { return mk<V>(a.y, -a.x); }
 template <typename V> __device__ __forceinline__ V cmul_pi(V a) { return mk<V>(-a.y, a.x); }

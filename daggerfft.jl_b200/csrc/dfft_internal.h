@@ -85,6 +85,8 @@ struct SlabKernel {
   int dflt; // an untuned plan may pick this variant
   const void* fn;      // forward
   const void* fn_inv;  // inverse
+  const void* fn_split;      // forward, rank-split layouts
+  const void* fn_inv_split;  // inverse, rank-split layouts
 };
 // Variant `v` (0-based) for (dbl, L), or null past the last one.
 const SlabKernel* find_slab_kernel(int dbl, int L, int v = 0);

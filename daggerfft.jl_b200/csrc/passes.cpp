@@ -1001,6 +1001,13 @@ Pass make_slab_split_pass(int dbl, int L, long long nslab, int inverse, int v, i
   g.rin = rin;
   g.rout = rout;
   g.zr = zr;
+  const SlabKernel* k = find_slab_kernel(dbl, L, v);
+  p.fn = inverse ? k->fn_inv_split : k->fn_split;
+  cuda_check(ensure_smem_attr(p.fn, p.smem), "cudaFuncSetAttribute(slab split)");
+  int occ = 0;
+  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p.fn, (int)p.block.x, p.smem),
+             "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (occ < 1) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "slab split kernel cannot be resident"};
   p.tL = rout;
   p.tO = zmax;
   return p;

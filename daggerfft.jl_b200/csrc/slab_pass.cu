@@ -2,20 +2,26 @@
 // planner chooses from.  The radices are those of the static plan for the
 // same length (the stage twiddle table is built from them); the planner
 // checks that they agree.
+// the fused slab pass is issue-bound: packed FP32 adds for its butterflies
+#define DFFT_PACKED_F32 1
 #include "dfft_internal.h"
 
 namespace dfft {
 
-#define DFFT_SLAB_INST1(T, LB, MINB, NB, DIR, L, P, CS, ...)                                          \
-  template __global__ void slab_xy_pass<T, LB, MINB, NB, DIR, L, P, CS, __VA_ARGS__>(                \
+#define DFFT_SLAB_INST1(T, LB, MINB, NB, DIR, SPLIT, L, P, CS, ...)                                   \
+  template __global__ void slab_xy_pass<T, LB, MINB, NB, DIR, SPLIT, L, P, CS, __VA_ARGS__>(         \
       const PassDesc, const PassDesc, const __grid_constant__ CUtensorMap, const SlabGeom);
-#define DFFT_SLAB_INST(T, LB, MINB, NB, L, P, CS, ...)            \
-  DFFT_SLAB_INST1(T, LB, MINB, NB, 1, L, P, CS, __VA_ARGS__)       \
-  DFFT_SLAB_INST1(T, LB, MINB, NB, 2, L, P, CS, __VA_ARGS__)
-// forward and inverse kernels of one launch shape
-#define K(T, LB, MINB, NB, L, P, CS, ...)                                     \
-  (const void*)&slab_xy_pass<T, LB, MINB, NB, 1, L, P, CS, __VA_ARGS__>,     \
-      (const void*)&slab_xy_pass<T, LB, MINB, NB, 2, L, P, CS, __VA_ARGS__>
+#define DFFT_SLAB_INST(T, LB, MINB, NB, L, P, CS, ...)                   \
+  DFFT_SLAB_INST1(T, LB, MINB, NB, 1, false, L, P, CS, __VA_ARGS__)       \
+  DFFT_SLAB_INST1(T, LB, MINB, NB, 2, false, L, P, CS, __VA_ARGS__)       \
+  DFFT_SLAB_INST1(T, LB, MINB, NB, 1, true, L, P, CS, __VA_ARGS__)        \
+  DFFT_SLAB_INST1(T, LB, MINB, NB, 2, true, L, P, CS, __VA_ARGS__)
+// forward and inverse kernels of one launch shape, plain then rank-split
+#define K(T, LB, MINB, NB, L, P, CS, ...)                                            \
+  (const void*)&slab_xy_pass<T, LB, MINB, NB, 1, false, L, P, CS, __VA_ARGS__>,     \
+      (const void*)&slab_xy_pass<T, LB, MINB, NB, 2, false, L, P, CS, __VA_ARGS__>, \
+      (const void*)&slab_xy_pass<T, LB, MINB, NB, 1, true, L, P, CS, __VA_ARGS__>,  \
+      (const void*)&slab_xy_pass<T, LB, MINB, NB, 2, true, L, P, CS, __VA_ARGS__>
 
 // threads = CS*P stage threads + one producer warp; MINB = CTAs per SM that
 // the NB tile buffers of CS*L elements leave room for

@@ -134,6 +134,13 @@ template <int R, int... Rest> struct first_radix { static constexpr int value = 
 __device__ __forceinline__ long long split_row(int R, long long zr, long long z, int y) {
   return (long long)(y % R) + (long long)R * (z + zr * (long long)(y / R));
 }
+// The same for the kernel's two forms: SPLIT = false is the plain layout
+// (row z * L + y, no run-time division), SPLIT = true reads R from g.
+template <bool SPLIT, int L>
+__device__ __forceinline__ long long slab_row(int R, long long zr, long long z, int y) {
+  if constexpr (SPLIT) return split_row(R, zr, z, y);
+  else return z * L + y;
+}
 
 // dx: x-phase descriptor (in -> out, contiguous pencils, FAST_IO global
 // stores); dy: y-phase descriptor (scale / inverse of the second axis).
@@ -143,7 +150,9 @@ __device__ __forceinline__ long long split_row(int R, long long zr, long long z,
 // records (byte 80); stage twiddles; NB tile buffers.
 // MINB: CTAs per SM the tile buffers allow (register budget per thread).
 // DIR: 1 forward, 2 inverse (compiled in: no per-element direction tests).
-template <typename T, int LB, int MINB, int NB, int DIR, int L, int P, int CS, int... Rs>
+// SPLIT: the rank-split layouts of SlabGeom (false: the plain layout, the
+// rin / rout / zr fields unused).
+template <typename T, int LB, int MINB, int NB, int DIR, bool SPLIT, int L, int P, int CS, int... Rs>
 __global__ void __launch_bounds__(LB, MINB)
     slab_xy_pass(const PassDesc dx, const PassDesc dy, const __grid_constant__ CUtensorMap tout,
                  const SlabGeom g) {
@@ -203,8 +212,11 @@ __global__ void __launch_bounds__(LB, MINB)
           const V* buf = bufs + b * bst;
           for (int kb = 0; kb < g.nlb; ++kb) {
             const int y = kb * g.lb;  // boxes never straddle a rank's rows (lb divides rout)
-            tma_store_3d(&tout, buf + (size_t)kb * g.lb * CS, tileb[b] * CS * g.xscale, y % g.rout,
-                         (int)(slabb[b] + g.zr * (y / g.rout)));
+            if constexpr (SPLIT)
+              tma_store_3d(&tout, buf + (size_t)kb * g.lb * CS, tileb[b] * CS * g.xscale, y % g.rout,
+                           (int)(slabb[b] + g.zr * (y / g.rout)));
+            else
+              tma_store_3d(&tout, buf + (size_t)kb * g.lb * CS, tileb[b] * CS * g.xscale, y, slabb[b]);
           }
           bulk_commit();
           bulk_wait_read_all();
@@ -265,14 +277,17 @@ __global__ void __launch_bounds__(LB, MINB)
         mbar_expect_tx(&full[b], tile_bytes);
         if (J.kind == 1) {
           // CS divides rin: the tile's CS pencils are contiguous in both layouts
-          bulk_load_1d(buf, reinterpret_cast<const V*>(dx.in.p) + split_row(g.rin, g.zr, J.slab, J.tile * CS) * L,
+          bulk_load_1d(buf, reinterpret_cast<const V*>(dx.in.p) + slab_row<SPLIT, L>(g.rin, g.zr, J.slab, J.tile * CS) * L,
                        tile_bytes, &full[b]);
         } else {
           fence_proxy_async_global();  // x-phase writes (generic proxy) before these async-proxy reads
           for (int kb = 0; kb < g.nlb; ++kb) {
             const int y = kb * g.lb;
-            tma_load_3d(buf + (size_t)kb * g.lb * CS, &tout, &full[b], J.tile * CS * g.xscale, y % g.rout,
-                        (int)(J.slab + g.zr * (y / g.rout)));
+            if constexpr (SPLIT)
+              tma_load_3d(buf + (size_t)kb * g.lb * CS, &tout, &full[b], J.tile * CS * g.xscale, y % g.rout,
+                          (int)(J.slab + g.zr * (y / g.rout)));
+            else
+              tma_load_3d(buf + (size_t)kb * g.lb * CS, &tout, &full[b], J.tile * CS * g.xscale, y, J.slab);
           }
         }
         kindb[b] = J.kind;
@@ -309,7 +324,7 @@ __global__ void __launch_bounds__(LB, MINB)
         const int t = tid % P, c = tid / P;
         const StrideCol<V> dense{buf + (size_t)c * L, 1};
         const XSwzCol<V, L, R0> sw{buf + (size_t)c * L, c};
-        const long long ob = split_row(g.rout, g.zr, J.slab, J.tile * CS + c) * L;
+        const long long ob = slab_row<SPLIT, L>(g.rout, g.zr, J.slab, J.tile * CS + c) * L;
         static_stages<T, L, P, true, 2, NC, DIR, 1, 1, 0, StrideCol<V>, XSwzCol<V, L, R0>, XSwzCol<V, L, R0>,
                       TWT, Rs...>(dx, t, dense, sw, sw, tw, 0, ob, true);
         fence_proxy_async_global();  // these stores are read by bulk-tensor loads
