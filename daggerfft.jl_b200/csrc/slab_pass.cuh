@@ -206,7 +206,17 @@ __global__ void __launch_bounds__(LB, MINB)
       auto settle = [&](int b) -> bool {
         if (kindb[b] == 0) return true;
         if (!mbar_wait_bounded(&empty[b], (uint32_t)((fills[b] - 1) & 1))) return false;
-        if (kindb[b] == 1) {  // release: the stage threads' stores, seen through the barrier, first
+        if (kindb[b] == 1) {
+          // the transformed pencils, contiguous in the output (CS divides
+          // rout): one bulk store, complete before the tile is published
+          // (async-proxy writes, made visible to the generic release by the
+          // proxy fence; readers fence again before their tensor loads)
+          const V* buf = bufs + b * bst;
+          V* dst = reinterpret_cast<V*>(dx.out.p) + slab_row<SPLIT, L>(g.rout, g.zr, slabb[b], tileb[b] * CS) * L;
+          bulk_store_1d(dst, buf, tile_bytes);
+          bulk_commit();
+          bulk_wait_all();
+          fence_proxy_async_global();
           asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(g.done + slabb[b]) : "memory");
         } else {
           const V* buf = bufs + b * bst;
@@ -321,13 +331,13 @@ __global__ void __launch_bounds__(LB, MINB)
       if (J.kind == 0) break;
       V* buf = bufs + b * bst;
       if (J.kind == 1) {
+        // pencils in place: dense in, swizzled between stages, dense out
+        // (the producer bulk-stores the tile)
         const int t = tid % P, c = tid / P;
         const StrideCol<V> dense{buf + (size_t)c * L, 1};
         const XSwzCol<V, L, R0> sw{buf + (size_t)c * L, c};
-        const long long ob = slab_row<SPLIT, L>(g.rout, g.zr, J.slab, J.tile * CS + c) * L;
-        static_stages<T, L, P, true, 2, NC, DIR, 1, 1, 0, StrideCol<V>, XSwzCol<V, L, R0>, XSwzCol<V, L, R0>,
-                      TWT, Rs...>(dx, t, dense, sw, sw, tw, 0, ob, true);
-        fence_proxy_async_global();  // these stores are read by bulk-tensor loads
+        static_stages<T, L, P, true, 1, NC, DIR, 1, 1, 0, StrideCol<V>, XSwzCol<V, L, R0>, StrideCol<V>,
+                      TWT, Rs...>(dx, t, dense, sw, dense, tw, 0, 0, true);
       } else {
         const int c = tid % CS, t = tid / CS;
         const StrideColC<V, CS> dense{buf + c};
