@@ -48,11 +48,11 @@ int dfft_plan_create(dfft_plan* plan, int ndim, const int64_t* shape, int precis
 }
 
 int dfft_slab_split_create(dfft_plan* plan, int precision, int inverse, int64_t L, int64_t nslab, int64_t zr,
-                           int nranks, unsigned flags) {
+                           int nranks, int split_dim, unsigned flags) {
   return guarded([&] {
     if (!plan) throw Error{DFFT_ERROR_INVALID_VALUE, "plan is NULL"};
     *plan = nullptr;
-    dfft::Plan* p = dfft::build_slab_split_plan(precision, inverse ? 1 : 0, L, nslab, zr, nranks, flags);
+    dfft::Plan* p = dfft::build_slab_split_plan(precision, inverse ? 1 : 0, L, nslab, zr, nranks, split_dim, flags);
     *plan = new dfft_plan_s{p};
   });
 }

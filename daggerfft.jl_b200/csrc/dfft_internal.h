@@ -71,6 +71,13 @@ struct Pass {
   size_t ctr_bytes = 0;  // job and per-slab counters (in the plan workspace)
   PassDesc d2{};
   SlabGeom sgeom{};
+  // slab pass with the y-phase first and columns split by rank (kernel
+  // MODE 2): the y-phase reads `in` through a map {tI2, tL2, tO2} and writes
+  // the plain intermediate {L, L, nslab} (in `in` when cols_mid_in, else
+  // in `out`), which the x-phase then reads
+  bool cols = false;
+  bool cols_mid_in = false;
+  long long tI2 = 0, tL2 = 0, tO2 = 0;
   std::vector<std::shared_ptr<DevTable>> tables;
 };
 
@@ -85,8 +92,10 @@ struct SlabKernel {
   int dflt; // an untuned plan may pick this variant
   const void* fn;      // forward
   const void* fn_inv;  // inverse
-  const void* fn_split;      // forward, rank-split layouts
-  const void* fn_inv_split;  // inverse, rank-split layouts
+  const void* fn_split;      // forward, rows split by rank
+  const void* fn_inv_split;  // inverse, rows split by rank
+  const void* fn_cols;       // forward, y-phase first, columns split by rank
+  const void* fn_inv_cols;   // inverse, the same
 };
 // Variant `v` (0-based) for (dbl, L), or null past the last one.
 const SlabKernel* find_slab_kernel(int dbl, int L, int v = 0);
@@ -114,8 +123,11 @@ Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v = 0);
 // The same pass over nslab slabs with rank-split input (rin rows per rank)
 // and/or output (rout rows per rank), zr slabs between one rank's blocks
 // (SlabGeom); rin = rout = L is make_slab_pass.
+// split_dim 2: rows (y) split, x-phase first (MODE 1); split_dim 1: columns
+// (x) split, y-phase first (MODE 2; rin / rout count columns, and the
+// forward pass overwrites its input with the intermediate).
 Pass make_slab_split_pass(int dbl, int L, long long nslab, int inverse, int v, int rin, int rout,
-                          long long zr);
+                          long long zr, int split_dim = 2);
 
 // Fused variant to use for dims (1, 2) of an L x L x O array, or -1 for the
 // per-axis passes `split` (x then y, already planned): wisdom, then timing

@@ -34,7 +34,7 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
 // The fused 2-D slab pass of a distributed Slab transform with the output
 // (forward) or input (inverse) in the rank-split layout (dfft_slab_split_create).
 Plan* build_slab_split_plan(int precision, int inverse, int64_t L, int64_t nslab, int64_t zr, int nranks,
-                            unsigned flags);
+                            int split_dim, unsigned flags);
 
 // work / chirp: workspaces supplied by the caller for this execution (null:
 // the plan's own); a plan built with kFlagCallerWorkspace owns none.

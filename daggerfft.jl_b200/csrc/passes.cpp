@@ -198,19 +198,24 @@ static cudaError_t encode_real_map(CUtensorMap* m, void* base, const Pass& p, in
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-static cudaError_t encode_map(CUtensorMap* m, void* base, const Pass& p) {
+static cudaError_t encode_map_dims(CUtensorMap* m, void* base, const Pass& p, long long tI, long long tL,
+                                   long long tO) {
   std::call_once(g_encode_once, load_encode);
   if (!g_encode) return cudaErrorNotSupported;
   const cuuint64_t esz = 8;
   const cuuint64_t xs = (cuuint64_t)p.geom.xscale;
-  cuuint64_t dims[3] = {(cuuint64_t)p.tI * xs, (cuuint64_t)p.tL, (cuuint64_t)p.tO};
-  cuuint64_t strides[2] = {(cuuint64_t)p.tI * xs * esz, (cuuint64_t)p.tI * xs * esz * (cuuint64_t)p.tL};
+  cuuint64_t dims[3] = {(cuuint64_t)tI * xs, (cuuint64_t)tL, (cuuint64_t)tO};
+  cuuint64_t strides[2] = {(cuuint64_t)tI * xs * esz, (cuuint64_t)tI * xs * esz * (cuuint64_t)tL};
   cuuint32_t box[3] = {(cuuint32_t)(p.geom.C * p.geom.xscale), (cuuint32_t)p.geom.lb, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+static cudaError_t encode_map(CUtensorMap* m, void* base, const Pass& p) {
+  return encode_map_dims(m, base, p, p.tI, p.tL, p.tO);
 }
 
 // Tensor map over {I, L, O} ComplexF32 (8-byte elements) with boxes of 16
@@ -977,8 +982,52 @@ Pass make_slab_pass(int dbl, int L, long long O, int inverse, int v) {
   return p;
 }
 
+// Columns split by rank, y-phase first (kernel MODE 2): the y-phase reads
+// the input through a map over its rank blocks of rin columns, the x-phase
+// writes pieces of rout elements (both powers of two, multiples of the tile
+// width); rin = L / rout = L is the plain side.
+static Pass make_slab_cols_pass(int dbl, int L, long long nslab, int inverse, int v, int rin, int rout,
+                                long long zr) {
+  Pass p = make_slab_pass(dbl, L, nslab, inverse, v);
+  SlabGeom& g = p.sgeom;
+  const int cs = p.geom.C;
+  auto pow2 = [](int x) { return x >= 1 && (x & (x - 1)) == 0; };
+  if (!pow2(rin) || !pow2(rout) || rin > L || rout > L || L % rin || L % rout || zr < nslab)
+    throw Error{DFFT_ERROR_INVALID_VALUE, "column split: columns per rank must be a power of two dividing L, zr >= slabs"};
+  if (rin % cs != 0 || rout % cs != 0)
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "column split: columns per rank do not hold whole tiles"};
+  const size_t esz = dbl ? 16 : 8;
+  if (((size_t)rout * esz) % 16 != 0 || ((size_t)rin * esz) % 16 != 0)
+    throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "column split: rows of a rank block are not 16-byte multiples"};
+  const long long zin = zr * (long long)(L / rin - 1) + nslab;
+  const long long zout = zr * (long long)(L / rout - 1) + nslab;
+  if (zin >= (1LL << 31) || zout >= (1LL << 31)) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "column split too large"};
+  g.rin = rin;
+  g.rout = rout;
+  g.zr = zr;
+  const SlabKernel* k = find_slab_kernel(dbl, L, v);
+  p.fn = inverse ? k->fn_inv_cols : k->fn_cols;
+  cuda_check(ensure_smem_attr(p.fn, p.smem), "cudaFuncSetAttribute(slab cols)");
+  int occ = 0;
+  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p.fn, (int)p.block.x, p.smem),
+             "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (occ < 1) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "slab column-split kernel cannot be resident"};
+  p.cols = true;
+  // forward: the intermediate overwrites the (plain) input; inverse: it
+  // goes to the (plain) output
+  p.cols_mid_in = !inverse;
+  p.tI = L;  // tout: the plain intermediate
+  p.tL = L;
+  p.tO = nslab;
+  p.tI2 = rin;  // tin: the input, rin columns per rank block
+  p.tL2 = L;
+  p.tO2 = zin;
+  return p;
+}
+
 Pass make_slab_split_pass(int dbl, int L, long long nslab, int inverse, int v, int rin, int rout,
-                          long long zr) {
+                          long long zr, int split_dim) {
+  if (split_dim == 1) return make_slab_cols_pass(dbl, L, nslab, inverse, v, rin, rout, zr);
   Pass p = make_slab_pass(dbl, L, nslab, inverse, v);
   SlabGeom& g = p.sgeom;
   const int cs = p.geom.C;
@@ -1089,17 +1138,26 @@ cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream,
     if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
       return cudaErrorMisalignedAddress;
     if (!work || (reinterpret_cast<uintptr_t>(work) & 7)) return cudaErrorInvalidValue;
-    CUtensorMap tout;
+    CUtensorMap tin, tout;
+    std::memset(&tin, 0, sizeof(tin));
     std::memset(&tout, 0, sizeof(tout));
-    e = encode_map(&tout, out, p);
+    void* mid = p.cols && p.cols_mid_in ? in : out;  // what tout covers
+    e = encode_map_dims(&tout, mid, p, p.tI, p.tL, p.tO);
     if (e != cudaSuccess) return e;
+    if (p.cols) {
+      e = encode_map_dims(&tin, in, p, p.tI2, p.tL2, p.tO2);
+      if (e != cudaSuccess) return e;
+      d.in.p = mid;  // the x-phase reads the intermediate
+    } else {
+      tin = tout;
+    }
     e = cudaMemsetAsync(work, 0, p.ctr_bytes, stream);
     if (e != cudaSuccess) return e;
     PassDesc d2 = p.d2;
     SlabGeom g = p.sgeom;
     g.jobs = static_cast<unsigned long long*>(work);
     g.done = reinterpret_cast<unsigned*>(static_cast<char*>(work) + 8);
-    void* args[] = {&d, &d2, &tout, &g};
+    void* args[] = {&d, &d2, &tin, &tout, &g};
     return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
   }
   if (p.pipe) {

@@ -321,7 +321,8 @@ Plan* build_plan(int ndim, const int64_t* shape, int precision, int transform, i
 }
 
 Plan* build_slab_split_plan(int precision, int inverse, int64_t L, int64_t nslab, int64_t zr, int nranks,
-                            unsigned flags) {
+                            int split_dim, unsigned flags) {
+  if (split_dim != 1 && split_dim != 2) throw Error{DFFT_ERROR_INVALID_VALUE, "split_dim must be 1 or 2"};
   if (precision != DFFT_F32 && precision != DFFT_F64)
     throw Error{DFFT_ERROR_INVALID_VALUE, "precision must be DFFT_F32 or DFFT_F64"};
   if (L < 1 || L > 0x7fffffffLL || nslab < 1 || zr < nslab || nranks < 1 || L % nranks != 0)
@@ -339,7 +340,8 @@ Plan* build_slab_split_plan(int precision, int inverse, int64_t L, int64_t nslab
   cuda_check(cudaGetDevice(&P->device), "cudaGetDevice");
   P->in_elem = P->out_elem = dbl ? 16 : 8;
   const int64_t plain[3] = {L, L, nslab};
-  const int64_t split[3] = {L, R, zr * (nranks - 1) + nslab};  // the span of the rank blocks
+  // the span of the rank blocks: rows (split_dim 2) or columns split
+  const int64_t split[3] = {split_dim == 2 ? L : R, split_dim == 2 ? R : L, zr * (nranks - 1) + nslab};
   for (int i = 0; i < 3; ++i) {
     P->in_shape[i] = inverse ? split[i] : plain[i];
     P->out_shape[i] = inverse ? plain[i] : split[i];
@@ -350,7 +352,7 @@ Plan* build_slab_split_plan(int precision, int inverse, int64_t L, int64_t nslab
   for (int v = 0; const SlabKernel* k = find_slab_kernel(dbl, (int)L, v); ++v) {
     if (!k->dflt) continue;
     try {
-      Pass p = make_slab_split_pass(dbl, (int)L, nslab, inverse, v, rin, rout, zr);
+      Pass p = make_slab_split_pass(dbl, (int)L, nslab, inverse, v, rin, rout, zr, split_dim);
       p.src = BUF_IN;
       p.dst = BUF_OUT;
       P->work_bytes = p.ctr_bytes;

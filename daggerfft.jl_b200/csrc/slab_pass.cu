@@ -8,20 +8,26 @@
 
 namespace dfft {
 
-#define DFFT_SLAB_INST1(T, LB, MINB, NB, DIR, SPLIT, L, P, CS, ...)                                   \
-  template __global__ void slab_xy_pass<T, LB, MINB, NB, DIR, SPLIT, L, P, CS, __VA_ARGS__>(         \
-      const PassDesc, const PassDesc, const __grid_constant__ CUtensorMap, const SlabGeom);
-#define DFFT_SLAB_INST(T, LB, MINB, NB, L, P, CS, ...)                   \
-  DFFT_SLAB_INST1(T, LB, MINB, NB, 1, false, L, P, CS, __VA_ARGS__)       \
-  DFFT_SLAB_INST1(T, LB, MINB, NB, 2, false, L, P, CS, __VA_ARGS__)       \
-  DFFT_SLAB_INST1(T, LB, MINB, NB, 1, true, L, P, CS, __VA_ARGS__)        \
-  DFFT_SLAB_INST1(T, LB, MINB, NB, 2, true, L, P, CS, __VA_ARGS__)
-// forward and inverse kernels of one launch shape, plain then rank-split
-#define K(T, LB, MINB, NB, L, P, CS, ...)                                            \
-  (const void*)&slab_xy_pass<T, LB, MINB, NB, 1, false, L, P, CS, __VA_ARGS__>,     \
-      (const void*)&slab_xy_pass<T, LB, MINB, NB, 2, false, L, P, CS, __VA_ARGS__>, \
-      (const void*)&slab_xy_pass<T, LB, MINB, NB, 1, true, L, P, CS, __VA_ARGS__>,  \
-      (const void*)&slab_xy_pass<T, LB, MINB, NB, 2, true, L, P, CS, __VA_ARGS__>
+#define DFFT_SLAB_INST1(T, LB, MINB, NB, DIR, MODE, L, P, CS, ...)                                    \
+  template __global__ void slab_xy_pass<T, LB, MINB, NB, DIR, MODE, L, P, CS, __VA_ARGS__>(          \
+      const PassDesc, const PassDesc, const __grid_constant__ CUtensorMap,                           \
+      const __grid_constant__ CUtensorMap, const SlabGeom);
+#define DFFT_SLAB_INST(T, LB, MINB, NB, L, P, CS, ...)              \
+  DFFT_SLAB_INST1(T, LB, MINB, NB, 1, 0, L, P, CS, __VA_ARGS__)      \
+  DFFT_SLAB_INST1(T, LB, MINB, NB, 2, 0, L, P, CS, __VA_ARGS__)      \
+  DFFT_SLAB_INST1(T, LB, MINB, NB, 1, 1, L, P, CS, __VA_ARGS__)      \
+  DFFT_SLAB_INST1(T, LB, MINB, NB, 2, 1, L, P, CS, __VA_ARGS__)      \
+  DFFT_SLAB_INST1(T, LB, MINB, NB, 1, 2, L, P, CS, __VA_ARGS__)      \
+  DFFT_SLAB_INST1(T, LB, MINB, NB, 2, 2, L, P, CS, __VA_ARGS__)
+// forward and inverse kernels of one launch shape: plain, rows split by
+// rank, columns split by rank (y-phase first)
+#define K(T, LB, MINB, NB, L, P, CS, ...)                                        \
+  (const void*)&slab_xy_pass<T, LB, MINB, NB, 1, 0, L, P, CS, __VA_ARGS__>,     \
+      (const void*)&slab_xy_pass<T, LB, MINB, NB, 2, 0, L, P, CS, __VA_ARGS__>, \
+      (const void*)&slab_xy_pass<T, LB, MINB, NB, 1, 1, L, P, CS, __VA_ARGS__>, \
+      (const void*)&slab_xy_pass<T, LB, MINB, NB, 2, 1, L, P, CS, __VA_ARGS__>, \
+      (const void*)&slab_xy_pass<T, LB, MINB, NB, 1, 2, L, P, CS, __VA_ARGS__>, \
+      (const void*)&slab_xy_pass<T, LB, MINB, NB, 2, 2, L, P, CS, __VA_ARGS__>
 
 // threads = CS*P stage threads + one producer warp; MINB = CTAs per SM that
 // the NB tile buffers of CS*L elements leave room for

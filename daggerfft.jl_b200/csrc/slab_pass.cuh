@@ -129,6 +129,20 @@ template <typename V, int CS, int R0> struct YSwzCol {
 };
 template <int R, int... Rest> struct first_radix { static constexpr int value = R; };
 
+// Tile buffer of CS pencils written in pieces of 2^rsh elements: element k
+// of pencil c at ((k >> rsh) * CS + c) * 2^rsh + (k mod 2^rsh), so piece s of
+// all CS pencils is one contiguous run (one bulk store per rank block).
+template <typename V> struct PieceCol {
+  V* p;  // the tile buffer
+  int c, cs, rsh;
+  __device__ __forceinline__ int at(int b, int off) const {
+    const int k = b + off;
+    return ((((k >> rsh) * cs) + c) << rsh) | (k & ((1 << rsh) - 1));
+  }
+  __device__ __forceinline__ V ld(int b, int off) const { return p[at(b, off)]; }
+  __device__ __forceinline__ void st(int b, int off, V v) const { p[at(b, off)] = v; }
+};
+
 // Row index (in units of L elements) of row y of slab z in a side with R
 // rows per rank (see SlabGeom).
 __device__ __forceinline__ long long split_row(int R, long long zr, long long z, int y) {
@@ -150,13 +164,26 @@ __device__ __forceinline__ long long slab_row(int R, long long zr, long long z, 
 // records (byte 80); stage twiddles; NB tile buffers.
 // MINB: CTAs per SM the tile buffers allow (register budget per thread).
 // DIR: 1 forward, 2 inverse (compiled in: no per-element direction tests).
-// SPLIT: the rank-split layouts of SlabGeom (false: the plain layout, the
-// rin / rout / zr fields unused).
-template <typename T, int LB, int MINB, int NB, int DIR, bool SPLIT, int L, int P, int CS, int... Rs>
+// MODE 0: x-phase then y-phase, plain layouts (the rin / rout / zr fields
+// unused; tin unused).  MODE 1: the same order, rows split by rank
+// (SlabGeom; the x-phase reads dx.in.p with rin and writes dx.out.p with
+// rout, the y-phase reads and writes through tout = the rout layout).
+// MODE 2: y-phase first, columns split by rank: the y-phase reads through
+// tin (the input; its x columns in blocks of rin per rank: column x of row
+// y of slab z at (x mod rin) + rin * (y + L * (z + zr * (x / rin)))) and
+// writes the plain intermediate through tout; the x-phase reads the
+// intermediate (dx.in.p) and writes dx.out.p in the same column-split
+// layout with rout (pieces of rout elements of each pencil, one block per
+// rank).  rin / rout = L is the plain layout.
+template <typename T, int LB, int MINB, int NB, int DIR, int MODE, int L, int P, int CS, int... Rs>
 __global__ void __launch_bounds__(LB, MINB)
-    slab_xy_pass(const PassDesc dx, const PassDesc dy, const __grid_constant__ CUtensorMap tout,
-                 const SlabGeom g) {
+    slab_xy_pass(const PassDesc dx, const PassDesc dy, const __grid_constant__ CUtensorMap tin,
+                 const __grid_constant__ CUtensorMap tout, const SlabGeom g) {
   typedef typename cvec<T>::type V;
+  constexpr bool SPLIT = MODE == 1;     // rows split by rank (x-phase first)
+  constexpr bool YX = MODE == 2;        // y-phase first, columns split by rank
+  constexpr int K1 = YX ? 2 : 1;        // job kind of the first phase
+  constexpr int K2 = YX ? 1 : 2;        // and of the second
   constexpr int NC = CS * P;  // stage threads
   static_assert(NC % 32 == 0 && NC + 32 == LB, "whole warps of stage threads plus one producer warp");
   static_assert(NB >= 2 && NB <= 4, "tile buffers");
@@ -206,20 +233,22 @@ __global__ void __launch_bounds__(LB, MINB)
       auto settle = [&](int b) -> bool {
         if (kindb[b] == 0) return true;
         if (!mbar_wait_bounded(&empty[b], (uint32_t)((fills[b] - 1) & 1))) return false;
-        if (kindb[b] == 1) {
+        const V* buf = bufs + b * bst;
+        if (kindb[b] == 1 && !YX) {
           // the transformed pencils, contiguous in the output (CS divides
-          // rout): one bulk store, complete before the tile is published
-          // (async-proxy writes, made visible to the generic release by the
-          // proxy fence; readers fence again before their tensor loads)
-          const V* buf = bufs + b * bst;
+          // rout): one bulk store
           V* dst = reinterpret_cast<V*>(dx.out.p) + slab_row<SPLIT, L>(g.rout, g.zr, slabb[b], tileb[b] * CS) * L;
           bulk_store_1d(dst, buf, tile_bytes);
-          bulk_commit();
-          bulk_wait_all();
-          fence_proxy_async_global();
-          asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(g.done + slabb[b]) : "memory");
+        } else if (kindb[b] == 1) {
+          // pieces of rout elements of the CS pencils, one block per rank
+          // (the stage threads left piece s of every pencil together)
+          const int y0 = tileb[b] * CS;
+          const uint32_t piece = (uint32_t)((size_t)CS * g.rout * sizeof(V));
+          for (int s = 0; s * g.rout < L; ++s)
+            bulk_store_1d(reinterpret_cast<V*>(dx.out.p) +
+                              (long long)g.rout * (y0 + (long long)L * (slabb[b] + g.zr * s)),
+                          buf + (size_t)s * CS * g.rout, piece);
         } else {
-          const V* buf = bufs + b * bst;
           for (int kb = 0; kb < g.nlb; ++kb) {
             const int y = kb * g.lb;  // boxes never straddle a rank's rows (lb divides rout)
             if constexpr (SPLIT)
@@ -228,8 +257,17 @@ __global__ void __launch_bounds__(LB, MINB)
             else
               tma_store_3d(&tout, buf + (size_t)kb * g.lb * CS, tileb[b] * CS * g.xscale, y, slabb[b]);
           }
-          bulk_commit();
-          bulk_wait_read_all();
+        }
+        bulk_commit();
+        if (kindb[b] == K1) {
+          // a first-phase tile: complete before it is published (async-proxy
+          // writes, made visible to the generic release by the proxy fence;
+          // readers fence again before their bulk / tensor loads)
+          bulk_wait_all();
+          fence_proxy_async_global();
+          asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(g.done + slabb[b]) : "memory");
+        } else {
+          bulk_wait_read_all();  // the buffer is free once the store has read it
         }
         kindb[b] = 0;
         return true;
@@ -261,20 +299,20 @@ __global__ void __launch_bounds__(LB, MINB)
           const long long i = (long long)(n % (2ull * Tt));
           if (i < Tt) {
             if (r >= g.nslab) continue;
-            J = SlabJob{1, (int)r, (int)i, 0};
+            J = SlabJob{K1, (int)r, (int)i, 0};
           } else {
             const long long sl = r - g.lag;
             if (sl < 0 || sl >= g.nslab) continue;
-            J = SlabJob{2, (int)sl, (int)(i - Tt), 0};
+            J = SlabJob{K2, (int)sl, (int)(i - Tt), 0};
           }
           break;
         }
-        if (J.kind == 2 && ld_acquire_gpu(g.done + J.slab) < (unsigned)Tt) {
-          // x-tiles of that slab may sit in this CTA's other buffers:
-          // publish them first
+        if (J.kind == K2 && ld_acquire_gpu(g.done + J.slab) < (unsigned)Tt) {
+          // first-phase tiles of that slab may sit in this CTA's other
+          // buffers: publish them first
           bool ok = true;
           for (int bb = 0; bb < NB; ++bb)
-            if (kindb[bb] == 1) ok = settle(bb) && ok;
+            if (kindb[bb] == K1) ok = settle(bb) && ok;
           if (!ok || !wait_slab(J.slab)) { failed = true; J.kind = 0; }
         }
         s_job[b] = J;
@@ -286,11 +324,21 @@ __global__ void __launch_bounds__(LB, MINB)
         V* buf = bufs + b * bst;
         mbar_expect_tx(&full[b], tile_bytes);
         if (J.kind == 1) {
-          // CS divides rin: the tile's CS pencils are contiguous in both layouts
-          bulk_load_1d(buf, reinterpret_cast<const V*>(dx.in.p) + slab_row<SPLIT, L>(g.rin, g.zr, J.slab, J.tile * CS) * L,
+          // CS divides rin: the tile's CS pencils are contiguous in both
+          // layouts (MODE 2: the plain intermediate the y-phase wrote)
+          if constexpr (YX) fence_proxy_async_global();  // after the acquire, before these async reads
+          bulk_load_1d(buf, reinterpret_cast<const V*>(dx.in.p) +
+                                (YX ? ((long long)J.slab * L + (long long)J.tile * CS)
+                                    : slab_row<SPLIT, L>(g.rin, g.zr, J.slab, J.tile * CS)) * L,
                        tile_bytes, &full[b]);
+        } else if constexpr (YX) {
+          // columns x0.. of the input, in the rank block holding them
+          const int x0 = J.tile * CS;
+          for (int kb = 0; kb < g.nlb; ++kb)
+            tma_load_3d(buf + (size_t)kb * g.lb * CS, &tin, &full[b], (x0 % g.rin) * g.xscale, kb * g.lb,
+                        (int)(J.slab + g.zr * (x0 / g.rin)));
         } else {
-          fence_proxy_async_global();  // x-phase writes (generic proxy) before these async-proxy reads
+          fence_proxy_async_global();  // after the acquire, before these async-proxy reads
           for (int kb = 0; kb < g.nlb; ++kb) {
             const int y = kb * g.lb;
             if constexpr (SPLIT)
@@ -304,8 +352,8 @@ __global__ void __launch_bounds__(LB, MINB)
         slabb[b] = J.slab;
         tileb[b] = J.tile;
       }
-      // publish the x-tiles and store the y-tiles still held by this CTA
-      // (on the error path too: other CTAs may wait for these x-tiles)
+      // publish the first-phase tiles and store the others still held by
+      // this CTA (on the error path too: other CTAs may wait for them)
       for (int bb = 0; bb < NB; ++bb)
         if (!settle(bb)) failed = true;
       if (failed && *verr == 0) atomicExch(g.err, DFFT_DEVERR_TMA_TIMEOUT);
@@ -336,8 +384,15 @@ __global__ void __launch_bounds__(LB, MINB)
         const int t = tid % P, c = tid / P;
         const StrideCol<V> dense{buf + (size_t)c * L, 1};
         const XSwzCol<V, L, R0> sw{buf + (size_t)c * L, c};
-        static_stages<T, L, P, true, 1, NC, DIR, 1, 1, 0, StrideCol<V>, XSwzCol<V, L, R0>, StrideCol<V>,
-                      TWT, Rs...>(dx, t, dense, sw, dense, tw, 0, 0, true);
+        if constexpr (YX) {
+          // out in pieces of rout elements, piece s of every pencil together
+          const PieceCol<V> pc{buf, c, CS, __ffs(g.rout) - 1};
+          static_stages<T, L, P, true, 1, NC, DIR, 1, 1, 0, StrideCol<V>, XSwzCol<V, L, R0>, PieceCol<V>,
+                        TWT, Rs...>(dx, t, dense, sw, pc, tw, 0, 0, true);
+        } else {
+          static_stages<T, L, P, true, 1, NC, DIR, 1, 1, 0, StrideCol<V>, XSwzCol<V, L, R0>, StrideCol<V>,
+                        TWT, Rs...>(dx, t, dense, sw, dense, tw, 0, 0, true);
+        }
       } else {
         const int c = tid % CS, t = tid / CS;
         const StrideColC<V, CS> dense{buf + c};

@@ -377,8 +377,9 @@ def _inplace(t):
 def _fused_slab(ws: Workspace, Az: DArray, By: DArray, transforms, dims, group, inverse):
     """The fused Slab exchange (dfft.slab_dist) for this pair of layouts, or
     None: L x L x N3 complex chunks on CUDA, one z-block per rank in A
-    (Blocks(L, L, ceil(N3 / P))), one y-block per rank in B
-    (Blocks(L, L / P, N3)), dims (1, 2, 3), FFT / IFFT tags."""
+    (Blocks(L, L, ceil(N3 / P))), one x-block (Blocks(L / P, L, N3), the
+    reference's Slab layout) or y-block (Blocks(L, L / P, N3)) per rank in
+    B, dims (1, 2, 3), FFT / IFFT tags."""
     fam = (IFFT, IFFT_) if inverse else (FFT, FFT_)
     if tuple(dims) != (1, 2, 3) or not all(isinstance(t, fam) for t in transforms):
         return None
@@ -394,13 +395,18 @@ def _fused_slab(ws: Workspace, Az: DArray, By: DArray, transforms, dims, group, 
             world = dist.get_world_size(group)
     except Exception:
         return None
-    if n1 % world or tuple(Az.blocks.b) != (n1, n2, -(-n3 // world)) or \
-            tuple(By.blocks.b) != (n1, n1 // world, n3):
+    if n1 % world or tuple(Az.blocks.b) != (n1, n2, -(-n3 // world)):
+        return None
+    if tuple(By.blocks.b) == (n1 // world, n1, n3):
+        split = "x"
+    elif tuple(By.blocks.b) == (n1, n1 // world, n3):
+        split = "y"
+    else:
         return None
     chunks = [c for c in Az.chunks if c is not None] + [c for c in By.chunks if c is not None]
     if not chunks or not all(c.is_cuda for c in chunks):
         return None
-    key = ("fused_slab", n1, n3, Az.dtype, world, rank)
+    key = ("fused_slab", n1, n3, Az.dtype, world, rank, split)
     cached = getattr(ws, "_fused", None)
     if cached is not None and cached[0] == key:
         return cached[1]
@@ -408,8 +414,8 @@ def _fused_slab(ws: Workspace, Az: DArray, By: DArray, transforms, dims, group, 
     try:
         # every rank (one without slabs too) builds a split plan now, so an
         # unsupported length falls back on all ranks before any exchange
-        SlabSplitPlan(n1, 1, 1, world, Az.dtype, inverse, chunks[0].device)
-        fs = FusedSlabFFT(n1, n3, Az.dtype, rank, world, group=group, device=chunks[0].device)
+        SlabSplitPlan(n1, 1, 1, world, Az.dtype, inverse, chunks[0].device, 1 if split == "x" else 2)
+        fs = FusedSlabFFT(n1, n3, Az.dtype, rank, world, group=group, device=chunks[0].device, split=split)
     except ArgumentError:
         return None
     ws._fused = (key, fs)

@@ -9,12 +9,16 @@ last-axis stage.  Here, for an L x L x N3 complex array with L divisible by
 the number of ranks P:
 
 * rank r holds the z-slabs Z_r (contiguous, ``zsplit``) as an F-ordered
-  (L, L, |Z_r|) array A_r, and receives the y-rows Y_r = [r R, (r+1) R),
-  R = L / P, of every slab as an F-ordered (L, R, N3) array B_r;
-* the fused slab pass writes its output in the rank-split layout
-  (``dfft_slab_split_create``): the rows rank s owns, of every local slab,
-  form one contiguous block -- exactly what rank s receives from r, and
-  exactly the slab range Z_r of B_s.  No pack or unpack kernel runs;
+  (L, L, |Z_r|) array A_r, and receives either the x-columns X_r = [r R,
+  (r+1) R), R = L / P, of every slab as an F-ordered (R, L, N3) array B_r
+  (split "x": the reference's Blocks(L, L, c) -> Blocks(c, L, N3)) or the
+  y-rows Y_r as an (L, R, N3) array (split "y");
+* the fused slab pass writes its output in a rank-split layout
+  (``dfft_slab_split_create``): the columns (rows) rank s owns, of every
+  local slab, form one contiguous block -- exactly what rank s receives
+  from r, and exactly the slab range Z_r of B_s.  No pack or unpack kernel
+  runs (for split "x" the slab pass runs its y-phase first and writes the
+  x-phase's pencils in per-rank pieces);
 * the local slabs run in ``ngroups`` groups; group g's blocks go out
   (NCCL grouped send/recv through ``torch.distributed``) while group g+1
   is still transforming, and the last-axis pass runs on B_r in place once
@@ -68,9 +72,15 @@ def groups_of(count: int, ngroups: int) -> List[Tuple[int, int]]:
 
 
 def split_row(R: int, zr: int, z: int, y: int) -> int:
-    """Row (units of L elements) of row y of local slab z in the rank-split
+    """Row (units of L elements) of row y of local slab z in the row-split
     layout with R rows per rank and zr slabs between rank blocks."""
     return (y % R) + R * (z + zr * (y // R))
+
+
+def split_col(R: int, L: int, zr: int, z: int, y: int, x: int) -> int:
+    """Element offset of (x, y, local slab z) in the column-split layout
+    with R columns per rank and zr slabs between rank blocks."""
+    return (x % R) + R * (y + L * (z + zr * (x // R)))
 
 
 def _flat(t: torch.Tensor) -> torch.Tensor:
@@ -92,20 +102,20 @@ class SlabSplitPlan:
     rank-split layout of ``nranks`` ranks, ``zr`` slabs between rank
     blocks.  ``execute`` takes flat tensors and element offsets."""
 
-    def __init__(self, L, nslab, zr, nranks, dtype, inverse, device=None):
+    def __init__(self, L, nslab, zr, nranks, dtype, inverse, device=None, split_dim=2):
         lib = _lib.lib()
         self._L = lib
         lib.dfft_slab_split_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
-                                               ctypes.c_uint]
+                                               ctypes.c_int, ctypes.c_uint]
         lib.dfft_slab_split_create.restype = ctypes.c_int
-        self.key = (L, nslab, zr, nranks, dtype, bool(inverse))
+        self.key = (L, nslab, zr, nranks, dtype, bool(inverse), split_dim)
         self.esz = torch.empty((), dtype=dtype).element_size()
         h = ctypes.c_void_p()
         dev = device if device is not None else torch.cuda.current_device()
         with torch.cuda.device(dev):
             check(lib.dfft_slab_split_create(ctypes.byref(h), _precision(dtype), 1 if inverse else 0,
-                                             L, nslab, zr, nranks, 0))
+                                             L, nslab, zr, nranks, split_dim, 0))
         self._h = h
 
     def execute(self, src: torch.Tensor, src_off: int, dst: torch.Tensor, dst_off: int, stream=None):
@@ -134,11 +144,12 @@ class CudaSlabKernels:
     def __init__(self):
         self._plans = {}
 
-    def slab(self, inverse, src, src_off, dst, dst_off, L, nslab, zr, nranks):
-        key = (L, nslab, zr, nranks, src.dtype, bool(inverse), src.device)
+    def slab(self, inverse, src, src_off, dst, dst_off, L, nslab, zr, nranks, split_dim=2):
+        key = (L, nslab, zr, nranks, src.dtype, bool(inverse), src.device, split_dim)
         p = self._plans.get(key)
         if p is None:
-            p = self._plans[key] = SlabSplitPlan(L, nslab, zr, nranks, src.dtype, inverse, src.device)
+            p = self._plans[key] = SlabSplitPlan(L, nslab, zr, nranks, src.dtype, inverse, src.device,
+                                                 split_dim)
         p.execute(src, src_off, dst, dst_off)
 
     def zpass(self, B: torch.Tensor, inverse: bool):
@@ -168,20 +179,27 @@ class FusedSlabFFT:
     z-slabs over ``world`` ranks (L % world == 0), with the pack and unpack
     of the exchange folded into the slab pass (module docstring).
 
-    ``forward(A, B)``: A = this rank's (L, L, |Z_r|) slab chunk (F-ordered,
-    transformed in place only in the sense that it is read), B = its
-    (L, L / world, N3) chunk of the result, written.  ``inverse(B, A)``:
-    the reverse (B is transformed in place along dim 3 first).  Every rank
-    calls the same methods in the same order.  ``exchange(ops, group)``
-    issues one batch of ("send" | "recv", tensor, peer) operations and
-    returns works to wait on (default: NCCL through torch.distributed)."""
+    ``split``: "x" -- B is split along dim 1, this rank's result chunk is
+    (L / world, L, N3) (the reference's Slab layouts, Blocks(L, L, c) to
+    Blocks(c, L, N3)); "y" -- split along dim 2, chunk (L, L / world, N3).
+    ``forward(A, B)``: A = this rank's (L, L, |Z_r|) slab chunk (F-ordered;
+    with split "x" it is overwritten, as the reference's in-place slab
+    stage overwrites it), B = its chunk of the result, written.
+    ``inverse(B, A)``: the reverse (B is transformed in place along dim 3
+    first).  Every rank calls the same methods in the same order.
+    ``exchange(ops, group)`` issues one batch of ("send" | "recv", tensor,
+    peer) operations and returns works to wait on (default: NCCL through
+    torch.distributed)."""
 
     def __init__(self, L: int, n3: int, dtype, rank: int, world: int, group=None, ngroups: int = 2,
-                 kernels=None, exchange=None, device=None):
+                 kernels=None, exchange=None, device=None, split: str = "x"):
         if world < 1 or L % world != 0:
             raise ArgumentError(_lib.ERROR_INVALID_VALUE, "fused Slab exchange needs L % ranks == 0")
         if ngroups < 1:
             raise ArgumentError(_lib.ERROR_INVALID_VALUE, "ngroups must be >= 1")
+        if split not in ("x", "y"):
+            raise ArgumentError(_lib.ERROR_INVALID_VALUE, 'split must be "x" or "y"')
+        self.split_dim = 1 if split == "x" else 2
         self.L, self.n3, self.dtype = int(L), int(n3), dtype
         self.rank, self.world, self.group = rank, world, group
         self.R = self.L // world
@@ -216,7 +234,8 @@ class FusedSlabFFT:
         for g in range(len(self.groups[r])):
             z0, n = self.groups[r][g]
             if n:
-                self.kernels.slab(False, Af, z0 * L * L, self.buf, z0 * L * R, L, n, self.Zr, P)
+                self.kernels.slab(False, Af, z0 * L * L, self.buf, z0 * L * R, L, n, self.Zr, P,
+                                  self.split_dim)
                 self.kernels.copy(self._col(Bf, r, z0, n), self._blk(r, z0, n))
             ops = []
             for s in range(P):
@@ -258,5 +277,6 @@ class FusedSlabFFT:
                 w.wait()
             z0, n = self.groups[r][g]
             if n:
-                self.kernels.slab(True, self.buf, z0 * L * R, Af, z0 * L * L, L, n, self.Zr, P)
+                self.kernels.slab(True, self.buf, z0 * L * R, Af, z0 * L * L, L, n, self.Zr, P,
+                                  self.split_dim)
         return A

@@ -108,23 +108,25 @@ function execute!(p::Plan, out::CuArray, in::CuArray)
 end
 
 """
-    slab_split_plan(T, L, nslab, zr, nranks; inverse=false)
+    slab_split_plan(T, L, nslab, zr, nranks; inverse=false, split_dim=1)
 
 The fused 2-D slab pass of a distributed Slab transform with the pack and
 unpack of the exchange folded in (`dfft_slab_split_create`): forward writes
-each rank's rows of every local slab as one contiguous block (the message
-to that rank), inverse reads the received blocks.  Run slab groups with
-`execute_split!` at element offsets; the blocks then go out with
-`MPI.Isend`/`MPI.Irecv!` and the received (L, L/P, N3) chunk takes a dims-3
-plan.
+each rank's columns (split_dim 1, the Blocks(L, L, c) -> Blocks(c, L, N3)
+layouts) or rows (split_dim 2) of every local slab as one contiguous block
+(the message to that rank), inverse reads the received blocks.  Run slab
+groups with `execute_split!` at element offsets; the blocks then go out
+with `MPI.Isend`/`MPI.Irecv!` and the received chunk takes a dims-3 plan.
+With split_dim 1 the forward overwrites its input, as the in-place slab
+stage does.
 """
 function slab_split_plan(::Type{T}, L::Integer, nslab::Integer, zr::Integer, nranks::Integer;
-                         inverse::Bool=false) where {T}
+                         inverse::Bool=false, split_dim::Integer=1) where {T}
     h = Ref{Ptr{Cvoid}}(C_NULL)
     check(ccall((:dfft_slab_split_create, libdfft), Cint,
-                (Ptr{Ptr{Cvoid}}, Cint, Cint, Int64, Int64, Int64, Cint, Cuint),
+                (Ptr{Ptr{Cvoid}}, Cint, Cint, Int64, Int64, Int64, Cint, Cint, Cuint),
                 h, precision_code(T), inverse ? Cint(1) : Cint(0), Int64(L), Int64(nslab), Int64(zr),
-                Cint(nranks), Cuint(0)))
+                Cint(nranks), Cint(split_dim), Cuint(0)))
     out = zeros(Int64, 3)
     check(ccall((:dfft_plan_output_shape, libdfft), Cint, (Ptr{Cvoid}, Ptr{Int64}), h[], out))
     Plan(h[], Tuple(out))

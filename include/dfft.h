@@ -125,21 +125,25 @@ DFFT_API int dfft_plan_create(dfft_plan* plan, int ndim, const int64_t* shape, i
  * (src/fftgpu.jl:324-415 gpu_flat_redistribute!, :417-480 pack_kernel! /
  * unpack_kernel!) next to the 2-D slab stage (src/fftgpu.jl:534-557 and
  * :596-619).  The plan runs the fused dims-(1, 2) pass over `nslab` L x L
- * slabs, one side in the RANK-SPLIT layout: with R = L / nranks rows per
- * rank, row y of slab z (L contiguous elements) sits at row
- *     (y mod R) + R * (z + zr * (y / R)),
- * so rank s's rows of every slab form one contiguous block of zr * R * L
- * elements (s = y / R).  Forward (inverse = 0): plain L x L x nslab input,
- * split output -- block s is what this rank sends to rank s, and the
- * blocks a rank receives, in sender order, are its (x, y in its rows, z)
- * array for the last-axis pass.  Inverse (inverse = 1): split input (the
- * received blocks), plain output.  zr >= nslab is the stride between rank
- * blocks in slabs: running slab groups z0.. of one local array means
+ * slabs, one side in a RANK-SPLIT layout with R = L / nranks:
+ *   split_dim = 1 (columns: the reference's Slab layouts, A = Blocks(L, L,
+ *     c), B = Blocks(L/P, L, N3)): element (x, y, z) of the local slabs at
+ *     (x mod R) + R * (y + L * (z + zr * (x / R))), so rank s = x / R gets
+ *     one contiguous (R, L, zr) block -- on arrival exactly its (R, L, N3)
+ *     chunk's z-range of the sender.  The y-phase runs first; the FORWARD
+ *     overwrites its input with the intermediate (as the reference's
+ *     in-place slab stage overwrites A).  R must be a power of two.
+ *   split_dim = 2 (rows, B = Blocks(L, L/P, N3)): row y of slab z (L
+ *     contiguous elements) at row (y mod R) + R * (z + zr * (y / R)).
+ * Forward (inverse = 0): plain L x L x nslab input, split output (block s
+ * is what this rank sends to rank s).  Inverse (inverse = 1): split input
+ * (the received blocks), plain output.  zr >= nslab is the stride between
+ * rank blocks in slabs: running slab groups z0.. of one local array means
  * offsetting the plain side by z0 * L * L and the split side by
  * z0 * R * L elements with the same zr.  Execute with dfft_execute.
  */
 DFFT_API int dfft_slab_split_create(dfft_plan* plan, int precision, int inverse, int64_t L, int64_t nslab,
-                                    int64_t zr, int nranks, unsigned flags);
+                                    int64_t zr, int nranks, int split_dim, unsigned flags);
 
 /* Output shape (column-major, ndim entries) of a plan. */
 DFFT_API int dfft_plan_output_shape(dfft_plan plan, int64_t* shape);
