@@ -1,8 +1,8 @@
 """Benchmark: 512^3 ComplexF32 C2C forward + inverse, Slab decomposition.
 
 One step = one forward 3-D FFT plus one inverse 3-D FFT of a 512^3
-ComplexF32 array (BASELINE config "3D C2C fft/ifft ComplexF32 512x512x512,
-iid standard-normal real/imag, decomp=Slab()"), inputs resident in HBM.
+ComplexF32 array (iid standard-normal real and imaginary parts,
+decomp=Slab()), inputs resident in HBM.
 
 value  : algorithmic GB/s = 2 transforms x 3 axis passes x (read + write of
          the 1 GiB field) = 12.885 GB per step, / step time, summed over ranks.

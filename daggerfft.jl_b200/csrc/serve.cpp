@@ -1,6 +1,6 @@
 // Serving runtime: continuous batching of transform requests on one GPU.
 //
-// No counterpart in the reference (north-star addition).  Requests arrive
+// No counterpart in the reference (an addition beyond its API).  Requests arrive
 // through dfft_server_submit from any thread.  A dispatcher thread admits
 // them in arrival order while a slot (an execution stream) is free and the
 // request's staging memory fits the HBM budget -- an arena carved once at

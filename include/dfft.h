@@ -197,7 +197,7 @@ DFFT_API int dfft_wisdom_size(int* n);
 
 /* ---- batches of uneven transforms -----------------------------------
  *
- * No counterpart in the reference (north-star addition): N independent
+ * No counterpart in the reference (an addition beyond its API): N independent
  * plans (any shapes/kinds) executed together.  By default the first execute
  * with a set of buffers captures every plan's passes as concurrent branches
  * of a CUDA graph (the branch count keeps the transforms in flight within
@@ -230,7 +230,7 @@ DFFT_API int dfft_batch_destroy(dfft_batch batch);
 
 /* ---- serving: continuous batching of transform requests --------------
  *
- * No counterpart in the reference (north-star addition).  A server owns an
+ * No counterpart in the reference (an addition beyond its API).  A server owns an
  * HBM arena of `hbm_budget_bytes` (allocated once) and `slots` execution
  * streams.  Requests are admitted in arrival order while a slot is free and
  * their staging memory (host input copied in, host or server-held output)
