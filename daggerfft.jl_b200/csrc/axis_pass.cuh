@@ -222,6 +222,16 @@ __device__ __forceinline__ typename cvec<T>::type load_raw(const IoAny& io, long
     }
     case IO_HERM_FULL: {
       const V* p = reinterpret_cast<const V*>(io.p);
+      if (io.t_m > 0) {
+        // sub-axis of a four-step pair: element kf of the whole axis, whose
+        // column starts j rows before b, rows t_i apart
+        const long long j = (b % io.t_ia) / io.t_i;
+        const long long kf = j + (long long)io.t_m * k;
+        const long long b0 = b - j * io.t_i;
+        if (kf == 0) return mk<V>(p[b0].x, z);
+        if (2 * kf <= io.n) return p[b0 + kf * io.t_i];
+        return cconj(p[b0 + (io.n - kf) * io.t_i]);
+      }
       if (k == 0) return mk<V>(p[b].x, z);  // c2r ignores Im X_0
       if (2 * k <= io.n) return p[b + k * io.sk];
       return cconj(p[b + (io.n - k) * io.sk]);
@@ -252,9 +262,12 @@ __device__ __forceinline__ void store_raw(const IoAny& io, long long b, int k,
     case IO_CPLX:
       reinterpret_cast<V*>(io.p)[b + k * io.sk] = cscale(v, s);
       return;
-    case IO_TRUNC:
-      if (k <= io.n) reinterpret_cast<V*>(io.p)[b + k * io.sk] = cscale(v, s);
+    case IO_TRUNC: {
+      // (a four-step sub-axis keeps the outputs whose whole-axis index fits)
+      const long long kf = io.t_m > 0 ? (b % io.t_ia) / io.t_i + (long long)io.t_m * k : (long long)k;
+      if (kf <= io.n) reinterpret_cast<V*>(io.p)[b + k * io.sk] = cscale(v, s);
       return;
+    }
     case IO_CPLX_TW: {
       const long long j = (b % io.t_ia) / io.t_i;
       const V w = ldg_c(reinterpret_cast<const V*>(io.w) +

@@ -1250,7 +1250,7 @@ static void four_step_pair(const PassSpec& s, int L1, int L2, Pass* pa, Pass* pb
   a.in.sk = s.I * L1;  // si = 1 and so as for the whole axis
   // sub-axis index j from the column base b = i + j I + o so: (b mod so) / I
   // (so need not be a multiple of I L1: Bluestein's input has L < L1 L2 rows)
-  if (a.in.chirp || a.in.mul) {
+  if (a.in.chirp || a.in.mul || a.in.kind == IO_HERM_FULL) {
     a.in.t_i = s.I;
     a.in.t_ia = a.in.so;
     a.in.t_m = L1;
@@ -1269,7 +1269,7 @@ static void four_step_pair(const PassSpec& s, int L1, int L2, Pass* pa, Pass* pb
   b.L = L1;
   b.I = s.I;
   b.O = (long long)L2 * s.O;
-  b.fast_io = !s.out.chirp;
+  b.fast_io = s.out.kind == IO_CPLX && !s.out.chirp;
   b.epi = false;
   b.C = 0;
   b.variant = four_step_factor(s.dbl, L1);
@@ -1282,7 +1282,7 @@ static void four_step_pair(const PassSpec& s, int L1, int L2, Pass* pa, Pass* pb
   b.out.so = s.I;
   b.out.o1 = L2;
   b.out.so2 = s.out.so;
-  if (b.out.chirp) {
+  if (b.out.chirp || b.out.kind == IO_TRUNC) {
     b.out.t_i = s.I;
     b.out.t_ia = s.out.so;
     b.out.t_m = L2;
@@ -1296,6 +1296,27 @@ static bool plain_complex_axis(const PassSpec& s) {
   return s.in.kind == IO_CPLX && s.out.kind == IO_CPLX && !s.epi && !s.in.chirp && !s.out.chirp &&
          !s.in.mul && s.in.o1 == 0 && s.out.o1 == 0 && s.in.si == 1 && s.out.si == 1 && s.in.sk == s.I &&
          s.out.sk == s.I && s.in.so == s.I * L && s.out.so == s.I * L;
+}
+
+// Sides a four-step pair can split: complex, or the full-length forms of
+// the real transforms (real in / first n+1 outputs kept; Hermitian half in
+// / real out), with unit inner stride and whole-axis columns.
+static bool four_step_sides(const PassSpec& s) {
+  const long long L = s.L;
+  auto ext_in = [&]() -> long long {
+    if (s.in.kind == IO_CPLX || s.in.kind == IO_REAL) return L;
+    if (s.in.kind == IO_HERM_FULL && s.in.n == L) return L / 2 + 1;
+    return -1;
+  };
+  auto ext_out = [&]() -> long long {
+    if (s.out.kind == IO_CPLX || s.out.kind == IO_REAL) return L;
+    if (s.out.kind == IO_TRUNC && s.out.n == L / 2) return L / 2 + 1;
+    return -1;
+  };
+  const long long ei = ext_in(), eo = ext_out();
+  return ei > 0 && eo > 0 && !s.epi && !s.in.chirp && !s.out.chirp && !s.in.mul && s.in.o1 == 0 &&
+         s.out.o1 == 0 && s.in.si == 1 && s.out.si == 1 && s.in.sk == s.I && s.out.sk == s.I &&
+         s.in.so == s.I * ei && s.out.so == s.I * eo;
 }
 
 static size_t add_four_step(std::vector<Pass>& out, const PassSpec& s, int L1, int L2, int src, int dst) {
@@ -1456,7 +1477,7 @@ size_t add_axis_passes(std::vector<Pass>& out, const PassSpec& s, unsigned flags
     if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
   }
   const int L = s.L;
-  if (plain_complex_axis(s)) {
+  if (four_step_sides(s)) {
     int L1 = 0, L2 = 0;
     if (four_step_split(s.dbl, L, &L1, &L2)) return add_four_step(out, s, L1, L2, src, dst);
   }
@@ -1511,7 +1532,11 @@ size_t add_axis_passes(std::vector<Pass>& out, const PassSpec& s, unsigned flags
     // S2 * Bhat -> S1 -> out * chirp.  The last pass's sub-axis index
     // k2 < M2 must stay below L (its column bases lie in the output).
     int M1 = 0, M2 = 0;
-    if (!plain_complex_axis(s) || !four_step_split(s.dbl, M, &M1, &M2) || M2 > L)
+    // the sub-axis index of a column must stay inside the column's extent
+    // on both sides (n1 < M1 rows of the input, k2 < M2 rows of the output)
+    const long long ein = s.in.kind == IO_HERM_FULL ? L / 2 + 1 : L;
+    const long long eout = s.out.kind == IO_TRUNC ? L / 2 + 1 : L;
+    if (!four_step_sides(s) || !four_step_split(s.dbl, M, &M1, &M2) || M2 > eout || M1 > ein)
       throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "length " + std::to_string(L) + " is too long for Bluestein here"};
     Pass p[4];
     four_step_pair(a, M1, M2, &p[0], &p[1]);

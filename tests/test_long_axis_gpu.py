@@ -96,3 +96,27 @@ def test_prime_long_axis_bluestein_over_four_step(dtype, shape, dims):
     _, B = _run(dfft.IFFT(), F, dims)
     assert rel(to_np(B), a) <= tol
     assert dfft.device_error() == 0
+
+
+@pytest.mark.parametrize("dtype,shape,dims", [
+    (np.float32, (1 << 20,), (1,)),          # full-length form over a 1024 x 1024 pair
+    (np.float64, (3, 131072), (2,)),         # strided, 256 x 512
+    (np.float32, (65536, 4, 3), (1, 2, 3)),  # long first axis, then the half spectrum
+    (np.float64, (100003,), (1,)),           # prime: Bluestein over four-step pairs
+    (np.float32, (99999,), (1,)),            # odd, 3^2 x 41 x 271: Bluestein, real sides
+])
+def test_long_real_axis_rfft_irfft(dtype, shape, dims):
+    # real transforms whose half length no single pass handles take the
+    # full-length form (real in, first n/2+1 outputs kept; Hermitian half
+    # in, real out), split into a four-step pair like a complex axis
+    a = rand(shape, dtype, seed=shape[0] % 89)
+    F = dfft.rfft(to_gpu(a), dims=dims)
+    ref = oracle.rfft(a, dims=dims)
+    tol = tol_for(dtype)
+    assert tuple(F.shape) == ref.shape
+    assert rel(to_np(F), ref) <= tol
+    d = shape[dims[0] - 1]
+    x = dfft.irfft(F, d, dims=dims)
+    assert rel(to_np(x), oracle.irfft(ref, d, dims=dims)) <= tol
+    assert rel(to_np(x), a) <= tol
+    assert dfft.device_error() == 0
