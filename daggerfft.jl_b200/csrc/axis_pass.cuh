@@ -239,16 +239,26 @@ __device__ __forceinline__ typename cvec<T>::type load_raw(const IoAny& io, long
     default: {  // IO_R2R
       const T* p = reinterpret_cast<const T*>(io.p);
       const V* w = reinterpret_cast<const V*>(io.w);
+      // a four-step sub-axis reads element kf of the whole axis (column
+      // base moved back by j rows, rows t_i apart)
+      long long bb = b, ss = io.sk;
+      int kk = k;
+      if (io.t_m > 0) {
+        const long long j = (b % io.t_ia) / io.t_i;
+        bb = b - j * io.t_i;
+        ss = io.t_i;
+        kk = (int)(j + (long long)io.t_m * k);
+      }
       switch (io.r2r) {
-        case K_REDFT10: return r2r_load<T, K_REDFT10>(p, b, io.sk, io.n, w, k);
-        case K_RODFT10: return r2r_load<T, K_RODFT10>(p, b, io.sk, io.n, w, k);
-        case K_REDFT01: return r2r_load<T, K_REDFT01>(p, b, io.sk, io.n, w, k);
-        case K_RODFT01: return r2r_load<T, K_RODFT01>(p, b, io.sk, io.n, w, k);
-        case K_REDFT11: return r2r_load<T, K_REDFT11>(p, b, io.sk, io.n, w, k);
-        case K_RODFT11: return r2r_load<T, K_RODFT11>(p, b, io.sk, io.n, w, k);
-        case K_REDFT00: return r2r_load<T, K_REDFT00>(p, b, io.sk, io.n, w, k);
-        case K_RODFT00: return r2r_load<T, K_RODFT00>(p, b, io.sk, io.n, w, k);
-        default: return r2r_load<T, K_DHT>(p, b, io.sk, io.n, w, k);
+        case K_REDFT10: return r2r_load<T, K_REDFT10>(p, bb, ss, io.n, w, kk);
+        case K_RODFT10: return r2r_load<T, K_RODFT10>(p, bb, ss, io.n, w, kk);
+        case K_REDFT01: return r2r_load<T, K_REDFT01>(p, bb, ss, io.n, w, kk);
+        case K_RODFT01: return r2r_load<T, K_RODFT01>(p, bb, ss, io.n, w, kk);
+        case K_REDFT11: return r2r_load<T, K_REDFT11>(p, bb, ss, io.n, w, kk);
+        case K_RODFT11: return r2r_load<T, K_RODFT11>(p, bb, ss, io.n, w, kk);
+        case K_REDFT00: return r2r_load<T, K_REDFT00>(p, bb, ss, io.n, w, kk);
+        case K_RODFT00: return r2r_load<T, K_RODFT00>(p, bb, ss, io.n, w, kk);
+        default: return r2r_load<T, K_DHT>(p, bb, ss, io.n, w, kk);
       }
     }
   }
@@ -288,16 +298,24 @@ __device__ __forceinline__ void store_raw(const IoAny& io, long long b, int k,
     default: {  // IO_R2R
       T* p = reinterpret_cast<T*>(io.p);
       const V* w = reinterpret_cast<const V*>(io.w);
+      long long bb = b, ss = io.sk;  // the whole axis, as for the load
+      int kk = k;
+      if (io.t_m > 0) {
+        const long long j = (b % io.t_ia) / io.t_i;
+        bb = b - j * io.t_i;
+        ss = io.t_i;
+        kk = (int)(j + (long long)io.t_m * k);
+      }
       switch (io.r2r) {
-        case K_REDFT10: r2r_store<T, K_REDFT10>(p, b, io.sk, io.n, w, k, v, s); return;
-        case K_RODFT10: r2r_store<T, K_RODFT10>(p, b, io.sk, io.n, w, k, v, s); return;
-        case K_REDFT01: r2r_store<T, K_REDFT01>(p, b, io.sk, io.n, w, k, v, s); return;
-        case K_RODFT01: r2r_store<T, K_RODFT01>(p, b, io.sk, io.n, w, k, v, s); return;
-        case K_REDFT11: r2r_store<T, K_REDFT11>(p, b, io.sk, io.n, w, k, v, s); return;
-        case K_RODFT11: r2r_store<T, K_RODFT11>(p, b, io.sk, io.n, w, k, v, s); return;
-        case K_REDFT00: r2r_store<T, K_REDFT00>(p, b, io.sk, io.n, w, k, v, s); return;
-        case K_RODFT00: r2r_store<T, K_RODFT00>(p, b, io.sk, io.n, w, k, v, s); return;
-        default: r2r_store<T, K_DHT>(p, b, io.sk, io.n, w, k, v, s); return;
+        case K_REDFT10: r2r_store<T, K_REDFT10>(p, bb, ss, io.n, w, kk, v, s); return;
+        case K_RODFT10: r2r_store<T, K_RODFT10>(p, bb, ss, io.n, w, kk, v, s); return;
+        case K_REDFT01: r2r_store<T, K_REDFT01>(p, bb, ss, io.n, w, kk, v, s); return;
+        case K_RODFT01: r2r_store<T, K_RODFT01>(p, bb, ss, io.n, w, kk, v, s); return;
+        case K_REDFT11: r2r_store<T, K_REDFT11>(p, bb, ss, io.n, w, kk, v, s); return;
+        case K_RODFT11: r2r_store<T, K_RODFT11>(p, bb, ss, io.n, w, kk, v, s); return;
+        case K_REDFT00: r2r_store<T, K_REDFT00>(p, bb, ss, io.n, w, kk, v, s); return;
+        case K_RODFT00: r2r_store<T, K_RODFT00>(p, bb, ss, io.n, w, kk, v, s); return;
+        default: r2r_store<T, K_DHT>(p, bb, ss, io.n, w, kk, v, s); return;
       }
     }
   }

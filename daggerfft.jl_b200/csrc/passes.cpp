@@ -1250,7 +1250,7 @@ static void four_step_pair(const PassSpec& s, int L1, int L2, Pass* pa, Pass* pb
   a.in.sk = s.I * L1;  // si = 1 and so as for the whole axis
   // sub-axis index j from the column base b = i + j I + o so: (b mod so) / I
   // (so need not be a multiple of I L1: Bluestein's input has L < L1 L2 rows)
-  if (a.in.chirp || a.in.mul || a.in.kind == IO_HERM_FULL) {
+  if (a.in.chirp || a.in.mul || a.in.kind == IO_HERM_FULL || a.in.kind == IO_R2R) {
     a.in.t_i = s.I;
     a.in.t_ia = a.in.so;
     a.in.t_m = L1;
@@ -1282,7 +1282,7 @@ static void four_step_pair(const PassSpec& s, int L1, int L2, Pass* pa, Pass* pb
   b.out.so = s.I;
   b.out.o1 = L2;
   b.out.so2 = s.out.so;
-  if (b.out.chirp || b.out.kind == IO_TRUNC) {
+  if (b.out.chirp || b.out.kind == IO_TRUNC || b.out.kind == IO_R2R) {
     b.out.t_i = s.I;
     b.out.t_ia = s.out.so;
     b.out.t_m = L2;
@@ -1298,25 +1298,37 @@ static bool plain_complex_axis(const PassSpec& s) {
          s.out.sk == s.I && s.in.so == s.I * L && s.out.so == s.I * L;
 }
 
-// Sides a four-step pair can split: complex, or the full-length forms of
-// the real transforms (real in / first n+1 outputs kept; Hermitian half in
-// / real out), with unit inner stride and whole-axis columns.
-static bool four_step_sides(const PassSpec& s) {
+// Sides a four-step pair can split, and the extents of their columns in
+// memory: complex, the full-length forms of the real transforms (real in /
+// first n/2+1 outputs kept; Hermitian half in / real out) and the r2r
+// kinds (n reals each side), with unit inner stride and whole-axis columns.
+// A sub-axis column index (n1 < L1 on the input, k2 < L2 on the output)
+// must stay inside its column's extent.
+static bool four_step_extents(const PassSpec& s, long long* ein, long long* eout) {
   const long long L = s.L;
-  auto ext_in = [&]() -> long long {
-    if (s.in.kind == IO_CPLX || s.in.kind == IO_REAL) return L;
-    if (s.in.kind == IO_HERM_FULL && s.in.n == L) return L / 2 + 1;
-    return -1;
+  auto ext = [&](const IoAny& io, bool out) -> long long {
+    switch (io.kind) {
+      case IO_CPLX:
+      case IO_REAL:
+        return L;
+      case IO_HERM_FULL:
+        return !out && io.n == L ? L / 2 + 1 : -1;
+      case IO_TRUNC:
+        return out && io.n == L / 2 ? L / 2 + 1 : -1;
+      case IO_R2R:
+        return io.n;
+      default:
+        return -1;
+    }
   };
-  auto ext_out = [&]() -> long long {
-    if (s.out.kind == IO_CPLX || s.out.kind == IO_REAL) return L;
-    if (s.out.kind == IO_TRUNC && s.out.n == L / 2) return L / 2 + 1;
-    return -1;
-  };
-  const long long ei = ext_in(), eo = ext_out();
-  return ei > 0 && eo > 0 && !s.epi && !s.in.chirp && !s.out.chirp && !s.in.mul && s.in.o1 == 0 &&
-         s.out.o1 == 0 && s.in.si == 1 && s.out.si == 1 && s.in.sk == s.I && s.out.sk == s.I &&
-         s.in.so == s.I * ei && s.out.so == s.I * eo;
+  const long long ei = ext(s.in, false), eo = ext(s.out, true);
+  if (ei <= 0 || eo <= 0 || s.epi || s.in.chirp || s.out.chirp || s.in.mul || s.in.o1 != 0 || s.out.o1 != 0 ||
+      s.in.si != 1 || s.out.si != 1 || s.in.sk != s.I || s.out.sk != s.I || s.in.so != s.I * ei ||
+      s.out.so != s.I * eo)
+    return false;
+  *ein = ei;
+  *eout = eo;
+  return true;
 }
 
 static size_t add_four_step(std::vector<Pass>& out, const PassSpec& s, int L1, int L2, int src, int dst) {
@@ -1477,9 +1489,11 @@ size_t add_axis_passes(std::vector<Pass>& out, const PassSpec& s, unsigned flags
     if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
   }
   const int L = s.L;
-  if (four_step_sides(s)) {
+  {
+    long long ein = 0, eout = 0;
     int L1 = 0, L2 = 0;
-    if (four_step_split(s.dbl, L, &L1, &L2)) return add_four_step(out, s, L1, L2, src, dst);
+    if (four_step_extents(s, &ein, &eout) && four_step_split(s.dbl, L, &L1, &L2) && L1 <= ein && L2 <= eout)
+      return add_four_step(out, s, L1, L2, src, dst);
   }
   if (L > (1 << 23)) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "length too large for Bluestein"};
   // the outer direction is in the tables; the inner FFT_M pair is forward
@@ -1534,9 +1548,8 @@ size_t add_axis_passes(std::vector<Pass>& out, const PassSpec& s, unsigned flags
     int M1 = 0, M2 = 0;
     // the sub-axis index of a column must stay inside the column's extent
     // on both sides (n1 < M1 rows of the input, k2 < M2 rows of the output)
-    const long long ein = s.in.kind == IO_HERM_FULL ? L / 2 + 1 : L;
-    const long long eout = s.out.kind == IO_TRUNC ? L / 2 + 1 : L;
-    if (!four_step_sides(s) || !four_step_split(s.dbl, M, &M1, &M2) || M2 > eout || M1 > ein)
+    long long ein = 0, eout = 0;
+    if (!four_step_extents(s, &ein, &eout) || !four_step_split(s.dbl, M, &M1, &M2) || M2 > eout || M1 > ein)
       throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "length " + std::to_string(L) + " is too long for Bluestein here"};
     Pass p[4];
     four_step_pair(a, M1, M2, &p[0], &p[1]);

@@ -120,3 +120,30 @@ def test_long_real_axis_rfft_irfft(dtype, shape, dims):
     assert rel(to_np(x), oracle.irfft(ref, d, dims=dims)) <= tol
     assert rel(to_np(x), a) <= tol
     assert dfft.device_error() == 0
+
+
+@pytest.mark.parametrize("kind,n,dtype,cols", [
+    (dfft.REDFT10, 65536, np.float64, 1),    # FFT length 65536: 256 x 256
+    (dfft.REDFT01, 40000, np.float32, 2),    # 200 x 200
+    (dfft.REDFT00, 20001, np.float64, 1),    # FFT length 40000
+    (dfft.RODFT00, 32767, np.float64, 1),    # FFT length 65536
+    (dfft.REDFT11, 30000, np.float32, 1),    # FFT length 60000
+    (dfft.RODFT11, 25000, np.float64, 1),    # FFT length 50000
+    (dfft.DHT, 50000, np.float64, 2),        # 5-smooth, 200 x 250
+    (dfft.RODFT10, 100003, np.float64, 1),   # prime: Bluestein over four-step pairs
+])
+def test_long_r2r_axis(kind, n, dtype, cols):
+    # r2r kinds on axes whose FFT no single pass handles: the loads and
+    # stores of the four-step sub-axes index the whole axis
+    a = rand((n, cols), dtype, seed=n % 97 + kind)
+    y = dfft.fft(to_gpu(a), dims=(1,), transforms=(dfft.R2R((kind,)),))
+    ref = oracle.r2r_1d(a.astype(np.float64), kind, 0)
+    assert rel(to_np(y), ref) <= tol_for(dtype)
+    assert dfft.device_error() == 0
+
+
+def test_long_r2r_strided_axis():
+    a = rand((3, 65536), np.float32, seed=11)
+    y = dfft.fft(to_gpu(a), dims=(2,), transforms=(dfft.R2R((dfft.REDFT10,)),))
+    ref = oracle.r2r_1d(a.astype(np.float64), dfft.REDFT10, 1)
+    assert rel(to_np(y), ref) <= 1e-5
