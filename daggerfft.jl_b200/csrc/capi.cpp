@@ -87,7 +87,8 @@ int dfft_plan_describe(dfft_plan plan, char* buf, size_t len) {
     if (!buf || len == 0) throw Error{DFFT_ERROR_INVALID_VALUE, "buf is NULL or len is 0"};
     std::string out;
     for (const dfft::Pass& q : p->passes) {
-      const char* kind = q.mixed ? (q.mstrided ? "mixed-strided" : "mixed-contig")
+      const char* kind = q.swap ? "axis-swap"
+                         : q.mixed ? (q.mstrided ? "mixed-strided" : "mixed-contig")
                          : q.slab ? "slab-xy" : q.feed ? "strided-feed" : q.async_ ? "strided-async"
                          : q.real ? "real-pipe"
                          : q.tiled == 1 ? "tiled-contig" : q.tiled == 2 ? "tiled-strided"
@@ -98,7 +99,8 @@ int dfft_plan_describe(dfft_plan plan, char* buf, size_t len) {
       if (q.mixed) rad = "32x16(tcgen05 fp16 hi+lo)";
       char line[256];
       // the two passes of a four-step axis: twiddled store, then the split output
-      const char* step = q.d.out.kind == dfft::IO_CPLX_TW ? " four-step=1" : q.d.out.o1 > 0 ? " four-step=2" : "";
+      const char* step = q.d.out.kind == dfft::IO_CPLX_TW || q.geom.tw_lo ? " four-step=1"
+                         : q.d.out.o1 > 0 || q.swap ? " four-step=2" : "";
       std::snprintf(line, sizeof line, "%s L=%d I=%lld O=%lld grid=%u block=%u smem=%zu radices=%s%s\n", kind,
                     q.d.L, q.d.I, q.d.I > 0 ? q.d.Q / q.d.I : 0LL, q.grid.x, q.block.x, q.smem,
                     rad.empty() ? "-" : rad.c_str(), step);

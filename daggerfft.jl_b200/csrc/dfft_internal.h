@@ -38,6 +38,13 @@ std::shared_ptr<DevTable> twiddle_table(int dbl, long long D, long long a, long 
 // One kernel launch of a plan.
 enum BufId : int { BUF_IN = 0, BUF_OUT = 1, BUF_WORK = 2, BUF_CHIRP = 3 };
 
+// Axis swap of the last four-step pass (transpose_pass.cu): element
+// (i, a, b, o) of an I x A x B x O array moves to (i, b, a, o).
+struct SwapGeom {
+  long long I, A, B, O;
+};
+const void* swap_axes_kernel(int dbl, bool tiled);
+
 struct Pass {
   PassDesc d{};
   const void* fn = nullptr;
@@ -75,6 +82,8 @@ struct Pass {
   // MODE 2): the y-phase reads `in` through a map {tI2, tL2, tO2} and writes
   // the plain intermediate {L, L, nslab} (in `in` when cols_mid_in, else
   // in `out`), which the x-phase then reads
+  bool swap = false;     // swap_axes_* (the last pass of a fast four-step axis)
+  SwapGeom swg{};
   bool cols = false;
   bool cols_mid_in = false;
   long long tI2 = 0, tL2 = 0, tO2 = 0;

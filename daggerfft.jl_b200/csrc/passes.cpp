@@ -1134,6 +1134,13 @@ cudaError_t launch_pass(const Pass& p, void* in, void* out, cudaStream_t stream,
     void* args[] = {&d, &tin, &tout, &g};
     return cudaLaunchKernel(p.fn, p.grid, p.block, args, p.smem, stream);
   }
+  if (p.swap) {
+    const void* a = in;
+    void* b = out;
+    SwapGeom g = p.swg;
+    void* args[] = {&a, &b, &g};
+    return cudaLaunchKernel(p.fn, p.grid, p.block, args, 0, stream);
+  }
   if (p.slab) {
     if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
       return cudaErrorMisalignedAddress;
@@ -1331,6 +1338,122 @@ static bool four_step_extents(const PassSpec& s, long long* ein, long long* eout
   return true;
 }
 
+// Axis swap pass (i, a, b, o) -> (i, b, a, o) over an I x A x B x O array.
+static Pass make_swap_pass(int dbl, long long I, long long A, long long B, long long O) {
+  Pass p;
+  p.swap = true;
+  p.swg = SwapGeom{I, A, B, O};
+  p.d.L = 1;
+  p.d.I = I;
+  p.d.Q = I * A * B * O;
+  p.fn = swap_axes_kernel(dbl, I == 1);
+  p.block = dim3(256);
+  const long long units = I == 1 ? ((A + 31) / 32) * ((B + 31) / 32) * O : (A * B * O + 7) / 8;
+  long long nb = (long long)sm_count() * 8;
+  if (nb > units) nb = units;
+  p.grid = dim3((unsigned)(nb > 0 ? nb : 1));
+  return p;
+}
+
+// The fast form of a plain complex four-step axis, three passes through one
+// scratch (the strided and contiguous passes keep their pipelined kernels):
+//   1. L2-point transforms along n2 (columns (i, n1), stride I L1) with the
+//      twiddle W_L^(n1 k2) applied to the transformed tile before its store;
+//   2. L1-point transforms along n1 (columns (i) per (k2, o), stride I), in
+//      place, leaving (i, k1, k2);
+//   3. the swap of the k1 and k2 axes into the output: (i, k2, k1), i.e.
+//      index k2 + L2 k1 along the axis.
+// Needs the pipelined strided kernel for L2 (else false, nothing added).
+// fast_split picks the largest strided factor with such a kernel (so the
+// contiguous factor is as short as it can be) whose cofactor is a length
+// one pass handles.
+static bool fast_split(int dbl, int L, int* Lc, int* Ls) {
+  for (int d = dbl ? 512 : 1024; d >= 2; --d) {
+    if (L % d != 0) continue;
+    const StaticPlan* sp = find_static(dbl, d);
+    if (!sp || !sp->pipe_s || sp->P > sp->lb) continue;
+    const int c = L / d;
+    // (a contiguous factor beyond one static plan runs the one-column
+    // dynamic kernel, slower than the two-pass form: 2^24 ComplexF32 1.28
+    // against 0.73 ms)
+    if (c < 2 || !four_step_factor(dbl, c)) continue;
+    *Ls = d;
+    *Lc = c;
+    return true;
+  }
+  return false;
+}
+
+static bool add_four_step_fast(std::vector<Pass>& out, const PassSpec& s, unsigned flags, int L1, int L2,
+                               int src, int dst) {
+  const long long L = (long long)L1 * L2;
+  PassSpec a;
+  a.dbl = s.dbl;
+  a.L = L2;
+  a.I = s.I * L1;
+  a.O = s.O;
+  a.inverse = s.inverse;
+  a.scale = 1.0;
+  a.in = s.in;
+  a.in.sk = s.I * L1;  // si = 1 and so = I L as for the whole axis
+  a.out = IoAny{};
+  a.out.kind = IO_CPLX;
+  a.out.si = 1;
+  a.out.sk = s.I * L1;
+  a.out.so = s.I * L;
+  a.fast_io = true;
+  a.variant = VARIANT_PIPE;
+  Pass pa;
+  try {
+    pa = make_pass(a);
+  } catch (const Error& e) {
+    if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE && e.status != DFFT_ERROR_INVALID_VALUE) throw;
+    return false;
+  }
+  if (!pa.tma || !pa.pipe) return false;  // the hook lives in the strided pipelined kernel
+  // W_L^m = W_L^(m mod B) * W_L^(B * (m / B)), two small tables
+  const int Bt = 1024;
+  auto lo = twiddle_table(s.dbl, L, 1, 0, Bt, s.inverse != 0);
+  auto hi = twiddle_table(s.dbl, L, Bt, 0, (int)((L + Bt - 1) / Bt), s.inverse != 0);
+  pa.tables.push_back(lo);
+  pa.tables.push_back(hi);
+  pa.geom.tw_lo = lo->p;
+  pa.geom.tw_hi = hi->p;
+  pa.geom.tw_div = s.I;
+  pa.geom.tw_lf = L;
+  pa.geom.tw_b = Bt;
+  PassSpec b;
+  b.dbl = s.dbl;
+  b.L = L1;
+  b.I = s.I;
+  b.O = (long long)L2 * s.O;
+  b.inverse = s.inverse;
+  b.scale = s.scale;
+  b.in.kind = b.out.kind = IO_CPLX;
+  b.in.si = b.out.si = 1;
+  b.in.sk = b.out.sk = s.I;
+  b.in.so = b.out.so = s.I * L1;
+  b.fast_io = true;
+  Pass pb;
+  try {
+    pb = plan_pass(b, flags);
+  } catch (const Error& e) {
+    if (e.status != DFFT_ERROR_UNSUPPORTED_SIZE) throw;
+    return false;
+  }
+  Pass pc = make_swap_pass(s.dbl, s.I, L1, L2, s.O);
+  pa.src = src;
+  pa.dst = BUF_CHIRP;
+  pb.src = BUF_CHIRP;
+  pb.dst = BUF_CHIRP;
+  pc.src = BUF_CHIRP;
+  pc.dst = dst;
+  out.push_back(std::move(pa));
+  out.push_back(std::move(pb));
+  out.push_back(std::move(pc));
+  return true;
+}
+
 static size_t add_four_step(std::vector<Pass>& out, const PassSpec& s, int L1, int L2, int src, int dst) {
   Pass pa, pb;
   four_step_pair(s, L1, L2, &pa, &pb);
@@ -1492,8 +1615,15 @@ size_t add_axis_passes(std::vector<Pass>& out, const PassSpec& s, unsigned flags
   {
     long long ein = 0, eout = 0;
     int L1 = 0, L2 = 0;
-    if (four_step_extents(s, &ein, &eout) && four_step_split(s.dbl, L, &L1, &L2) && L1 <= ein && L2 <= eout)
+    if (four_step_extents(s, &ein, &eout) && four_step_split(s.dbl, L, &L1, &L2) && L1 <= ein && L2 <= eout) {
+      // plain complex sides: the three-pass form (strided pass on a factor
+      // with a pipelined kernel, contiguous pass on its cofactor)
+      int Lc = 0, Ls = 0;
+      if (plain_complex_axis(s) && fast_split(s.dbl, L, &Lc, &Ls) &&
+          add_four_step_fast(out, s, flags, Lc, Ls, src, dst))
+        return (size_t)(s.I * s.O) * (size_t)L * (s.dbl ? 16 : 8);
       return add_four_step(out, s, L1, L2, src, dst);
+    }
   }
   if (L > (1 << 23)) throw Error{DFFT_ERROR_UNSUPPORTED_SIZE, "length too large for Bluestein"};
   // the outer direction is in the tables; the inner FFT_M pair is forward

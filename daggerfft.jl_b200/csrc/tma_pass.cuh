@@ -55,6 +55,13 @@ struct TmaGeom {
   int bstride;        // elements between tile buffers (a multiple of 128 bytes)
   unsigned tile_bytes;
   int* err;           // device error word
+  // strided variant, first pass of a four-step axis (null otherwise): row k
+  // of column q leaves times W_lf^((q / tw_div) * k), read from the two
+  // tables W_lf^(m mod tw_b) (tw_lo) and W_lf^(tw_b * (m / tw_b)) (tw_hi)
+  const void* tw_lo;
+  const void* tw_hi;
+  long long tw_div, tw_lf;
+  int tw_b;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -250,6 +257,21 @@ __global__ void __launch_bounds__(LB) axis_pass_pipe(const PassDesc d,
         const StrideCol<V> col{sb + c, C};
         static_stages<T, L, P, true, 1, 0, 0, 1, 1, 0, StrideCol<V>, StrideCol<V>, StrideCol<V>,
                       GlobalTw<V>, Rs...>(d, t, col, col, col, twl, 0, 0, true);
+      }
+      if (g.tw_lo) {
+        // the four-step twiddle on the transformed tile (row k at k * C + c;
+        // the stages ended with a barrier), then a barrier before the store
+        const V* lo = reinterpret_cast<const V*>(g.tw_lo);
+        const V* hi = reinterpret_cast<const V*>(g.tw_hi);
+        const long long q0 = (tile % g.tiles_i) * (long long)C;
+        for (int e = tid; e < C * L; e += blockDim.x) {
+          const int k = e / C;
+          const long long q = q0 + (e - k * C);
+          const long long m = ((q / g.tw_div) * (long long)k) % g.tw_lf;
+          const V w = cmul(ldg_c(lo + m % g.tw_b), ldg_c(hi + m / g.tw_b));
+          sb[e] = cmul(sb[e], w);
+        }
+        __syncthreads();
       }
     }
     fence_proxy_async_smem();

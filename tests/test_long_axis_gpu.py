@@ -147,3 +147,21 @@ def test_long_r2r_strided_axis():
     y = dfft.fft(to_gpu(a), dims=(2,), transforms=(dfft.R2R((dfft.REDFT10,)),))
     ref = oracle.r2r_1d(a.astype(np.float64), dfft.REDFT10, 1)
     assert rel(to_np(y), ref) <= 1e-5
+
+
+@pytest.mark.parametrize("dtype,shape,dims", [
+    (np.complex64, (1 << 20,), (1,)),
+    (np.complex64, (6, 65536), (2,)),        # strided: the swap moves rows of 6
+    (np.complex128, (1 << 18, 3), (1,)),
+])
+def test_long_axis_fast_form(dtype, shape, dims):
+    # plain complex long axes take the three-pass form: the strided pass
+    # (pipelined, twiddle on its tile), the contiguous pass, the axis swap
+    a = rand(shape, dtype, seed=len(shape))
+    p, F = _run(dfft.FFT(), to_gpu(a), dims)
+    desc = p.describe()
+    assert "axis-swap" in desc and "strided-pipe" in desc, desc
+    tol = tol_for(dtype)
+    assert rel(to_np(F), oracle.fft(a, dims=dims)) <= tol
+    _, B = _run(dfft.IFFT(), F, dims)
+    assert rel(to_np(B), a) <= tol
