@@ -625,6 +625,133 @@ function gpu_ifft!(A::ChunkedArray, B::ChunkedArray, wsBA, transforms, dims, ::S
     A
 end
 
+# ---- the Slab exchange with pack and unpack folded into the slab pass -----
+# (columns split by rank: the Blocks(L, L, c) -> Blocks(c, L, N3) layouts)
+
+"z-slab ranges (start, count) per rank: blocks of cld(n3, P), one per rank."
+slab_zsplit(n3, P) = [(min(r * cld(n3, P), n3), min(cld(n3, P), n3 - min(r * cld(n3, P), n3))) for r in 0:P-1]
+
+"Slab groups (offset, count) of `count` local slabs, the same rule on every rank."
+function slab_groups(count, ngroups)
+    count == 0 && return [(0, 0) for _ in 1:ngroups]
+    g = max(1, min(ngroups, count))
+    base, extra = divrem(count, g)
+    out = Tuple{Int,Int}[]
+    z = 0
+    for i in 0:ngroups-1
+        n = i < g ? base + (i < extra ? 1 : 0) : 0
+        push!(out, (z, n))
+        z += n
+    end
+    out
+end
+
+"""
+    fused_slab_fft!(Bloc, Aloc, L, n3, rank, nranks; comm=nothing, ngroups=2)
+
+Forward 3-D FFT of an L x L x n3 complex array distributed in z-slabs
+(`Aloc` = this rank's (L, L, |Z_r|) chunk, overwritten as the in-place
+slab stage overwrites it) into x-blocks (`Bloc` = its (L/P, L, n3) chunk)
+with no pack or unpack kernel: the slab pass writes each rank's columns of
+every local slab as one contiguous block (`slab_split_plan`), the blocks go
+out per slab group with MPI point-to-point (CUDA-aware) while the next group
+transforms, and the last-axis pass runs on `Bloc` in place.
+"""
+function fused_slab_fft!(Bloc::CuArray{T,3}, Aloc::CuArray{T,3}, L::Integer, n3::Integer, rank::Integer,
+                         nranks::Integer; comm=nothing, ngroups::Integer=2) where {T}
+    L % nranks == 0 || throw(ArgumentError("fused Slab exchange needs L % ranks == 0"))
+    R = L ÷ nranks
+    LR = L * R
+    zs = slab_zsplit(n3, nranks)
+    Zr = zs[rank+1][2]
+    groups = [slab_groups(zs[s+1][2], ngroups) for s in 1:nranks]
+    buf = CuArray{T}(undef, LR * Zr * nranks)
+    Bv = vec(Bloc)
+    mpi = comm === nothing ? nothing :
+          Base.require(Base.PkgId(Base.UUID("da04e1cc-30fd-572f-bb4f-1f8673147195"), "MPI"))
+    reqs = Any[]
+    for g in 1:ngroups
+        z0, n = groups[rank+1][g]
+        if n > 0
+            p = slab_split_plan(T, L, n, Zr, nranks; split_dim=1)
+            execute_split!(p, buf, z0 * LR, Aloc, z0 * L * L)
+            a = (rank * Zr + z0) * LR
+            b = (zs[rank+1][1] + z0) * LR
+            copyto!(view(Bv, b+1:b+n*LR), view(buf, a+1:a+n*LR))
+        end
+        CUDA.synchronize()  # the blocks are written before MPI reads them
+        for s in 0:nranks-1
+            (s == rank || mpi === nothing) && continue
+            zs0, ns = groups[s+1][g]
+            if ns > 0
+                b = (zs[s+1][1] + zs0) * LR
+                push!(reqs, mpi.Irecv!(view(Bv, b+1:b+ns*LR), comm; source=s, tag=g))
+            end
+            if n > 0
+                a = (s * Zr + z0) * LR
+                push!(reqs, mpi.Isend(view(buf, a+1:a+n*LR), comm; dest=s, tag=g))
+            end
+        end
+    end
+    isempty(reqs) || mpi.Waitall(mpi.RequestSet(reqs))
+    execute!(plan_transform(FFT!(), Bloc, (3,)), Bloc, Bloc)
+    Bloc
+end
+
+"""
+    fused_slab_ifft!(Aloc, Bloc, L, n3, rank, nranks; comm=nothing, ngroups=2)
+
+The inverse: the last-axis IFFT on `Bloc` in place, each owner's z-range of
+`Bloc` (contiguous) sent to it, and each group of local slabs transformed
+out of the received column blocks into `Aloc` as the group arrives.
+"""
+function fused_slab_ifft!(Aloc::CuArray{T,3}, Bloc::CuArray{T,3}, L::Integer, n3::Integer, rank::Integer,
+                          nranks::Integer; comm=nothing, ngroups::Integer=2) where {T}
+    L % nranks == 0 || throw(ArgumentError("fused Slab exchange needs L % ranks == 0"))
+    R = L ÷ nranks
+    LR = L * R
+    zs = slab_zsplit(n3, nranks)
+    Zr = zs[rank+1][2]
+    groups = [slab_groups(zs[s+1][2], ngroups) for s in 1:nranks]
+    buf = CuArray{T}(undef, LR * Zr * nranks)
+    Bv = vec(Bloc)
+    execute!(plan_transform(IFFT!(), Bloc, (3,)), Bloc, Bloc)
+    CUDA.synchronize()
+    mpi = comm === nothing ? nothing :
+          Base.require(Base.PkgId(Base.UUID("da04e1cc-30fd-572f-bb4f-1f8673147195"), "MPI"))
+    batches = Vector{Any}[]
+    for g in 1:ngroups
+        z0, n = groups[rank+1][g]
+        reqs = Any[]
+        for s in 0:nranks-1
+            (s == rank || mpi === nothing) && continue
+            zs0, ns = groups[s+1][g]
+            if n > 0
+                a = (s * Zr + z0) * LR
+                push!(reqs, mpi.Irecv!(view(buf, a+1:a+n*LR), comm; source=s, tag=g))
+            end
+            if ns > 0
+                b = (zs[s+1][1] + zs0) * LR
+                push!(reqs, mpi.Isend(view(Bv, b+1:b+ns*LR), comm; dest=s, tag=g))
+            end
+        end
+        if n > 0
+            a = (rank * Zr + z0) * LR
+            b = (zs[rank+1][1] + z0) * LR
+            copyto!(view(buf, a+1:a+n*LR), view(Bv, b+1:b+n*LR))
+        end
+        push!(batches, reqs)
+    end
+    for g in 1:ngroups
+        isempty(batches[g]) || mpi.Waitall(mpi.RequestSet(batches[g]))
+        z0, n = groups[rank+1][g]
+        n > 0 || continue
+        p = slab_split_plan(T, L, n, Zr, nranks; inverse=true, split_dim=1)
+        execute_split!(p, Aloc, z0 * L * L, buf, z0 * LR)
+    end
+    Aloc
+end
+
 "`gpu_cleanup_workspace!` (src/fftgpu.jl:630-634)."
 function gpu_cleanup_workspace!(ws::GPUWorkspace)
     ws.send_buffer = nothing
@@ -634,7 +761,7 @@ function gpu_cleanup_workspace!(ws::GPUWorkspace)
 end
 
 export fft, ifft, rfft, irfft, fft!, ifft!, apply_gpu_fft!, Pencil, Slab, R2R
-export slab_split_plan, execute_split!
+export slab_split_plan, execute_split!, fused_slab_fft!, fused_slab_ifft!
 export Batch, launches, wisdom_export, wisdom_import, wisdom_forget, wisdom_size, device_error
 export Server, submit, poll, release, cancel, stats, reset_stats!, serve
 export ChunkedArray, distribute, distribute_empty, create_gpu_workspace, gpu_coalesced_redistribute!,
