@@ -38,8 +38,9 @@ template <typename V, typename S> __device__ __forceinline__ V cscale(V a, S s) 
 // ComplexF32 adds and subtracts as packed two-lane FP32 instructions
 // (add / sub.rn.f32x2, sm_100; the same round-to-nearest sums as the scalar
 // form).  Half the issue slots for the butterflies: the fused slab pass,
-// bound by instruction issue, runs 9 % faster with them (512^3, B200); the
-// 1024-thread strided pass, bound by its barriers, runs 15 % slower.  A
+// bound by instruction issue, runs 9 % faster with them and the
+// producer-fed strided pass 3 % faster (512^3, B200); the 1024-thread
+// pipelined strided pass, bound by its barriers, runs 15 % slower.  A
 // translation unit opts in by defining DFFT_PACKED_F32 before including
 // this header.
 #ifdef DFFT_PACKED_F32

@@ -2,6 +2,8 @@
 // and its launch shapes, fastest first (B200, 512^3 / 256^3 / 128^3 arrays).
 // threads = CS*P stage threads + one producer warp; MINB = CTAs per SM that
 // NB tile buffers of CS*L elements leave room for.
+// the producer-fed strided pass: packed FP32 adds for its butterflies
+#define DFFT_PACKED_F32 1
 #include "dfft_internal.h"
 
 namespace dfft {
