@@ -208,6 +208,12 @@ class FusedSlabFFT:
         self.groups = [groups_of(self.zs[s][1], ngroups) for s in range(world)]
         self.kernels = kernels or CudaSlabKernels()
         self.exchange = exchange or _nccl_exchange
+        if exchange is None and world > 1:
+            # a collective first, so that every rank has joined the
+            # communicator before the point-to-point batches (a rank's first
+            # batch may be empty)
+            import torch.distributed as dist
+            dist.barrier(group=group)
         self.device = device
         # the split side of this rank's slab passes: every rank block of
         # every local slab (the send buffer forward, the receive buffer inverse)
