@@ -83,6 +83,7 @@ def test_long_axis_in_place():
     (np.complex64, (65537, 2), (1,)),      # M = 131220, two pencils
     (np.complex128, (3, 100003), (2,)),    # strided, M = 202500
     (np.complex64, (1000003,), (1,)),      # M = 2025000
+    (np.complex128, (1000003,), (1,)),     # M = 2025000, ComplexF64 factors <= 2048
 ])
 def test_prime_long_axis_bluestein_over_four_step(dtype, shape, dims):
     # a long prime axis: Bluestein's length-M convolution runs as two
@@ -104,6 +105,8 @@ def test_prime_long_axis_bluestein_over_four_step(dtype, shape, dims):
     (np.float32, (65536, 4, 3), (1, 2, 3)),  # long first axis, then the half spectrum
     (np.float64, (100003,), (1,)),           # prime: Bluestein over four-step pairs
     (np.float32, (99999,), (1,)),            # odd, 3^2 x 41 x 271: Bluestein, real sides
+    (np.float64, (1 << 20, 2), (1,)),        # Float64 full-length form, two columns
+    (np.float32, (5, 262144), (2,)),         # strided long real axis
 ])
 def test_long_real_axis_rfft_irfft(dtype, shape, dims):
     # real transforms whose half length no single pass handles take the
@@ -131,6 +134,9 @@ def test_long_real_axis_rfft_irfft(dtype, shape, dims):
     (dfft.RODFT11, 25000, np.float64, 1),    # FFT length 50000
     (dfft.DHT, 50000, np.float64, 2),        # 5-smooth, 200 x 250
     (dfft.RODFT10, 100003, np.float64, 1),   # prime: Bluestein over four-step pairs
+    (dfft.REDFT10, 65536, np.float32, 3),
+    (dfft.RODFT01, 36000, np.float32, 1),
+    (dfft.REDFT11, 70001, np.float64, 1),    # FFT length 140002 = 2 x 70001: Bluestein
 ])
 def test_long_r2r_axis(kind, n, dtype, cols):
     # r2r kinds on axes whose FFT no single pass handles: the loads and

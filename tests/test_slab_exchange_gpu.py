@@ -83,6 +83,7 @@ def _run_ranks(world, fn):
     (256, 30, 4, 2, np.complex64),     # uneven z-ranges (8, 8, 8, 6)
     (256, 20, 2, 2, np.complex128),
     (512, 3, 4, 2, np.complex64),      # a rank with no slabs
+    (512, 12, 2, 3, np.complex128),    # ComplexF64 L = 512 (16-byte elements, 8 x 8 x 8 slab kernel)
 ])
 def test_fused_slab_exchange_loopback(L, n3, world, ngroups, dtype, split):
     a = rand((L, L, n3), dtype, seed=L + n3 + world)
