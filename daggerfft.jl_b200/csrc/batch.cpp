@@ -17,6 +17,7 @@
 // if the topology changed, re-instantiate it.  Capture happens on a private
 // stream (capturing the legacy default stream is not allowed); the graph is
 // launched on the caller's stream.
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -117,8 +118,9 @@ Batch* build_batch(int n, const dfft_plan* plans, unsigned flags) {
   }
   if ((flags & DFFT_BATCH_PERSISTENT) && !(flags & DFFT_BATCH_GRAPH)) {
     // a pass is claimed about `lag` transforms after the one it depends on:
-    // the caller's (flag bits 8-15), else half the graph's branch count
-    // (transforms whose buffers fit L2 at once)
+    // the caller's (flag bits 8-15), else the graph's branch count
+    // (transforms whose buffers fit L2 at once), at least 4 (64 uneven
+    // ComplexF32 grids: lag 1 3.85 ms, 2 3.23, 4 2.91, 16 2.91, 64 2.92)
     const int user_lag = (int)((flags >> 8) & 0xFFu);
     double total = 0;
     for (const Plan* p : B->plans) total += (double)(p->in_bytes() + p->out_bytes());
@@ -127,7 +129,7 @@ Batch* build_batch(int n, const dfft_plan* plans, unsigned flags) {
       cudaGetLastError();
       l2 = 0;
     }
-    const int lag = user_lag > 0 ? user_lag : batch_branch_rule(n, total, l2, kBatchStreams) / 2;
+    const int lag = user_lag > 0 ? user_lag : std::max(4, batch_branch_rule(n, total, l2, kBatchStreams));
     B->persist = make_persistent_batch(B->plans, lag < 1 ? 1 : lag);
     if (B->persist) B->launches = 1;
   }
